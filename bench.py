@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Throughput of the MLS-MPM substep on B200: particle-updates/s at 1M
+particles (2048x512 grid, 999,424 particles, dt 5e-7), FP32 strain form and
+FP64 forms, through the C ABI of libicempm.so.
+
+One bench step = one icm_run_substeps call of --substeps substeps (default
+100; the hot path over the whole particle set, back to back as inside a
+frame). L2 is flushed (256 MB write) before every timed step. Timing: CUDA
+events on the library's stream, max over ranks.
+
+  python bench.py [--gpus N --steps K --warmup W]      our arm (FP32 headline)
+  python bench.py --impl reference                      CPU oracle arm
+
+Multi-GPU: replicas only (each rank runs the full workload on its own GPU;
+the substep has no cross-GPU exchange), scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-updates/s at 1M pts: FP32/learned vs plain FP64, 1 B200, ≤1% force err"
+UNIT = "particle-updates/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    a = argparse.ArgumentParser()
+    a.add_argument("--gpus", type=int, default=1)
+    a.add_argument("--steps", type=int, default=10)
+    a.add_argument("--warmup", type=int, default=3)
+    a.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    a.add_argument("--config", default="c3_1m")
+    a.add_argument("--substeps", type=int, default=100)
+    a.add_argument("--tile", type=int, default=-1, help="tile variant (-1: autotuned)")
+    a.add_argument("--threads", type=int, default=256)
+    a.add_argument("--no-e2e", action="store_true")
+    a.add_argument("--no-accuracy", action="store_true")
+    a.add_argument("--no-cpu", action="store_true")
+    a.add_argument("--no-fp64", action="store_true")
+    return a.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """Samples nvidia-smi every 200 ms while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_summary():
+    """Per-launch DRAM bytes of the fused kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def alg_bytes(form: str, n: int, na: int, ng: int) -> float:
+    """Algorithmic bytes of one steady-state substep launch.
+    fp32 fused: particle state read 36 B (cell 4, fraction 8, H 16, Jp 4,
+      meta 4) + written 28 B (cell, fraction, H); grid 48 B per active node
+      (read 16, scatter 16, zero 16).
+    fp64 fused: read 60 B (pos 16, Fe 32, Jp 8, meta 4) + written 48 B;
+      grid 96 B per active node.
+    fp64 stepwise (reference layout, three kernels): 260 B per particle +
+      32 B per node + 72 B per active node."""
+    if form == "fp32":
+        return 64.0 * n + 48.0 * na
+    if form == "fp64":
+        return 108.0 * n + 96.0 * na
+    return 260.0 * n + 32.0 * ng + 72.0 * na
+
+
+def cpu_oracle_rate(name: str, budget_s: float, max_substeps: int, threads: int):
+    """Particle-updates/s of the CPU FP64 oracle on the workload (a bounded
+    sample: substeps until the time budget is spent)."""
+    from icempm_b200 import configs
+    from oracle import oracle as orc
+
+    p, soa = configs.make_scene(name)
+    grid = orc.new_grid(p)
+    bins = np.zeros(2 * p.n_indenter_subdivisions)
+    orc.run_substeps(p, soa, grid, bins, 1, threads=threads, history=False)  # warm
+    done, t0 = 0, time.perf_counter()
+    while done < max_substeps:
+        orc.run_substeps(p, soa, grid, bins, 1, threads=threads, history=False)
+        done += 1
+        if time.perf_counter() - t0 > budget_s and done >= 2:
+            break
+    dt = time.perf_counter() - t0
+    return p.nPts * done / dt, done, dt, p.nPts
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from icempm_b200 import configs
+    from oracle import oracle as orc
+
+    threads = host_threads()
+    p, soa = configs.make_scene(args.config)
+    grid = orc.new_grid(p)
+    bins = np.zeros(2 * p.n_indenter_subdivisions)
+    sub = 2  # substeps per step: a bounded sample of the workload
+    for _ in range(args.warmup):
+        orc.run_substeps(p, soa, grid, bins, sub, threads=threads, history=False)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        orc.run_substeps(p, soa, grid, bins, sub, threads=threads, history=False)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = p.nPts * sub * args.steps / total
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.config}: 2D MLS-MPM ice indentation, {p.nPts} particles, "
+                               f"{p.GridX}x{p.GridY} grid, dt {p.InitialTimeStep:g}",
+                   "substeps_per_step": sub, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sub} substeps per step of the {p.nPts}-particle workload, "
+                                   f"FP64 CPU restatement of gpu_implementation5.cu, OpenMP {threads} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    import icempm_b200 as im
+    from icempm_b200 import configs
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    name = args.config
+    p0, soa0 = configs.make_scene(name)
+    n, ng = p0.nPts, p0.GridTotal
+    na = configs.active_nodes(p0, soa0)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def make(form, tile):
+        m = im.Model(local)
+        m.prms = configs.make_params(name)
+        m.gpu.model = m
+        gx, gy, dim, dt, cx, cy, _ = configs.CONFIGS[name]
+        m.load_block(cx, cy, 0.2, 0.05, 12345)
+        m.gpu.set_form(form)
+        m.gpu.set_tile(tile, args.threads)
+        return m
+
+    def timed(m, steps, warmup, substeps, ktime=False, clocks=None):
+        g = m.gpu
+        ext = torch.cuda.ExternalStream(g.stream_handle())
+        for _ in range(warmup):
+            g.run_substeps(m.prms, substeps)
+        g.synchronize()
+        if ktime:
+            g.kernel_timing(True)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        barrier()
+        torch.cuda.synchronize()
+        g.synchronize()
+        ctx = clocks if clocks is not None else _Null()
+        with ctx:
+            for k in range(steps):
+                with torch.cuda.stream(ext):
+                    flush.zero_()
+                evs[k][0].record(ext)
+                g.run_substeps(m.prms, substeps)
+                evs[k][1].record(ext)
+            g.synchronize()
+            torch.cuda.synchronize()
+        barrier()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        kt = g.kernel_time() if ktime else (0.0, 0)
+        if ktime:
+            g.kernel_timing(False)
+        return ms, kt
+
+    # --- tile choice (autotuner cache, else default)
+    tile = args.tile
+    tune_note = "fixed"
+    if tile < 0:
+        from icempm_b200 import autotune
+
+        tile, threads, tune_note = autotune.choose(name, im.FORM_FP32, local)
+        args.threads = threads
+
+    # --- headline: FP32 fused form
+    m = make(im.FORM_FP32, tile)
+    clocks = Clocks(local)
+    ms, (kms, klaunch) = timed(m, args.steps, args.warmup, args.substeps, ktime=True, clocks=clocks)
+    total_s = max_over_ranks(sum(ms) / 1e3)
+    value = world * n * args.substeps * args.steps / total_s
+    redo = m.gpu.fp64_redo_count()
+    m.gpu.close()
+
+    hbm, peak_kind = peaks()
+    kavg_s = (kms / klaunch / 1e3) if klaunch else float("nan")
+    ab = alg_bytes("fp32", n, na, ng)
+    achieved = ab / kavg_s / 1e9
+    tr = traffic_summary().get("fp32")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": tr, "kernel": "k_tile_substep<Pol32,...,kModeFull>", "alg_bytes_per_launch": ab,
+            "avg_launch_us": kavg_s * 1e6, "launches_timed": klaunch, "peak_kind": peak_kind}
+
+    extra = {}
+    # --- FP64 forms (the plain drop-in and the fused FP64 form)
+    if not args.no_fp64:
+        k2 = max(2, args.steps // 3)
+        for form, key in ((im.FORM_FP64, "fp64_fused"), (im.FORM_FP64_STEPWISE, "fp64_stepwise")):
+            mm = make(form, tile)
+            ms2, (k2ms, k2n) = timed(mm, k2, 1, args.substeps, ktime=(form == im.FORM_FP64))
+            t2 = max_over_ranks(sum(ms2) / 1e3)
+            v2 = world * n * args.substeps * k2 / t2
+            d = {"value": v2, "ms_per_step": sum(ms2) / k2, "steps": k2}
+            if k2n:
+                a2 = alg_bytes("fp64", n, na, ng) / (k2ms / k2n / 1e3) / 1e9
+                d["roofline"] = {"achieved": a2, "frac": a2 / hbm, "avg_launch_us": 1e3 * k2ms / k2n}
+            extra[key] = d
+            mm.gpu.close()
+        extra["speedup_fp32_vs_fp64_stepwise"] = value / extra["fp64_stepwise"]["value"]
+        extra["speedup_fp32_vs_fp64_fused"] = value / extra["fp64_fused"]["value"]
+
+    # --- accuracy of the FP32 form over a full 10,000-substep frame
+    if not args.no_accuracy and rank == 0:
+        nsub = configs.CONFIGS[name][6]
+        res = {}
+        for form in (im.FORM_FP64, im.FORM_FP32):
+            mm = make(form, tile)
+            mm.gpu.run_substeps(mm.prms, nsub)
+            hist = mm.gpu.force_history(nsub)
+            mm.gpu.cuda_transfer_from_device()
+            mm.gpu.synchronize()
+            res[form] = (hist, mm.gpu.tmp_transfer_buffer.copy(), mm.gpu.error_code)
+            mm.gpu.close()
+        h64, s64, e64 = res[im.FORM_FP64]
+        h32, s32, e32 = res[im.FORM_FP32]
+        f64 = np.hypot(h64[:, 0], h64[:, 1])
+        f32 = np.hypot(h32[:, 0], h32[:, 1])
+        pitch = int(p0.nPtsPitch)
+        x64 = s64[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n]
+        x32 = s32[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n]
+        extra["accuracy"] = {
+            "substeps": nsub, "against": "fp64 fused form on the GPU (parity-tested against the CPU FP64 oracle)",
+            "peak_force_fp64_N": float(f64.max()), "peak_force_fp32_N": float(f32.max()),
+            "peak_force_rel_err": float(abs(f32.max() - f64.max()) / max(f64.max(), 1e-30)),
+            "force_history_rel_l2": float(np.linalg.norm(f32 - f64) / max(np.linalg.norm(f64), 1e-30)),
+            "max_pos_err_h": float(np.abs(x32 - x64).max() / p0.cellsize),
+            "p99_pos_err_h": float(np.percentile(np.abs(x32 - x64).max(axis=0), 99) / p0.cellsize),
+            "error_flags": [int(e64), int(e32)],
+            "fp64_fallback_particles": redo,
+        }
+
+    # --- end to end: one frame through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        nsub = configs.CONFIGS[name][6]
+        mm = make(im.FORM_FP32, tile)
+        g = mm.gpu
+        host = g.tmp_transfer_buffer.copy()
+        bytes_soa = 8 * int(mm.prms.nPtsPitch) * 16
+        d2h = bytes_soa + 8 * 2 * mm.prms.n_indenter_subdivisions + 4
+        times = []
+        for k in range(1 + 2):
+            g.tmp_transfer_buffer[:] = host
+            barrier()
+            g.synchronize()
+            g.record_start()
+            g.transfer_ponts_to_device()
+            g.run_substeps(mm.prms, nsub)
+            g.cuda_transfer_from_device()
+            g.record_stop()
+            g.synchronize()
+            if k > 0:
+                times.append(g.elapsed_ms() / 1e3)
+        te = max_over_ranks(sum(times))
+        e2e = {"value": world * n * nsub * len(times) / te, "unit": UNIT, "h2d_bytes_per_step": bytes_soa,
+               "d2h_bytes_per_step": d2h, "substeps_per_step": nsub, "steps": len(times),
+               "what": "Model-level frame: H2D of the reference SoA from pinned memory, 10,000 substeps, "
+                       "D2H of SoA + force bins + error word"}
+        mm.gpu.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        thr = host_threads()
+        rate, done, secs, npts = cpu_oracle_rate(name, 10.0, 200, thr)
+        cpu = {"value": rate, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": f"{done} substeps ({secs:.1f} s) of the {npts}-particle workload, FP64 CPU restatement "
+                         f"of gpu_implementation5.cu (oracle/mpm_oracle.c), OpenMP {thr} threads"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sum(ms) / len(ms), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{name}: 2D MLS-MPM ice indentation, {n} particles, {p0.GridX}x{p0.GridY} grid "
+                                   f"(h = 1/{round(1 / p0.cellsize)} m), dt {p0.InitialTimeStep:g}, FP32 strain form",
+                       "substeps_per_step": args.substeps, "tile": im.TILE_VARIANTS[tile], "threads": args.threads,
+                       "tile_choice": tune_note, "active_nodes": na,
+                       "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
+            "gpu_launches": args.steps * (args.substeps + 1),
+            "roofline": roof,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+        }
+        out.update(extra)
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,816 @@
+// device_layer.cu -- the C ABI device layer (include/icempm.h).
+//
+// One icm_ctx replaces one GPU_Implementation5 (gpu_implementation5.h:40-72):
+// it owns a CUDA stream, two timing events, the reference-layout particle
+// SoA / grid / force bins, and -- for the fused forms -- the internal tile-
+// ordered particle arrays, three grid buffers and the binning scratch.
+//
+// Which copy of the particle state is current is tracked explicitly:
+//   ref_valid       the reference SoA on the device holds the state;
+//   internal_valid  the tile-ordered arrays hold the state.
+// Fused runs pack (bin + gather) from the reference SoA when needed and leave
+// the internal arrays current; member-style kernels and transfers unpack
+// first. Nothing here falls back to the host: every failure is a status.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <algorithm>
+#include <vector>
+
+#include "../../include/icempm.h"
+#include "errors.h"
+#include "k_stepwise.cuh"
+#include "k_tiles.cuh"
+
+using namespace icm;
+
+#define ICM_CUDA(call)                                                                                      \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess)                                                                              \
+            return icm::fail(ICM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));            \
+    } while (0)
+
+#define ICM_LAUNCHED(what)                                                                                  \
+    do {                                                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                                                \
+        if (e_ != cudaSuccess) return icm::fail(ICM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+struct TileVariant { int TX, TY; };
+constexpr TileVariant kVariants[4] = {{16, 8}, {16, 16}, {32, 8}, {32, 16}};
+
+template <class T>
+int dalloc(T **p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return icm::fail(ICM_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return ICM_OK;
+}
+
+template <class T>
+void dfree(T *&p)
+{
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+struct Binning {
+    int *key = nullptr, *count = nullptr, *cell_start = nullptr, *cursor = nullptr, *perm = nullptr;
+    int *chunk = nullptr, *tile_start = nullptr, *pid = nullptr;
+    size_t cap_pts = 0, cap_cells = 0, cap_tiles = 0;
+};
+
+struct Fused {
+    int form = -1;  // ICM_FORM_FP64 / ICM_FORM_FP32 held in these buffers
+    size_t cap_pts = 0, cap_nodes = 0, cap_tiles = 0;
+    Parts64 p64{};
+    Parts32 p32{};
+    void *grid[3] = {nullptr, nullptr, nullptr};
+    uint8_t *dirty = nullptr;  // 3 * cap_tiles
+};
+
+}  // namespace
+
+struct icm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    int form = ICM_FORM_FP64_STEPWISE;
+    int tile_variant = 1, threads = 256;
+
+    icy_SimParams prms{};
+    size_t cap_pts = 0, cap_nodes = 0, pts_pitch = 0, grid_pitch = 0;
+    double *d_pts = nullptr, *d_grid = nullptr, *d_bins = nullptr;
+    int *d_err = nullptr;
+    double *d_hist = nullptr;
+    size_t hist_cap = 0;
+    int hist_n = 0;
+    unsigned long long *d_redo = nullptr;
+
+    // optional per-launch timing of the fused substep kernel (kModeFull)
+    bool ktime = false;
+    std::vector<cudaEvent_t> kev;  // pairs
+    size_t kev_used = 0;
+    double ktime_ms = 0;
+    long long ktime_count = 0;
+
+    bool ref_valid = true, internal_valid = false, internal_pq = false;
+    int internal_variant = -1;
+    Binning bin;
+    Fused fz;
+};
+
+// ------------------------------------------------------------ helpers
+
+static int check_params(icm_ctx *c, const icy_SimParams *p)
+{
+    if (!c->d_pts) return icm::fail(ICM_ERR_STATE, "arrays are not allocated (call icm_allocate_arrays)");
+    if (p->nPts < 0 || (size_t)p->nPts > c->cap_pts)
+        return icm::fail(ICM_ERR_ARG, "nPts exceeds the allocated particle count");
+    if (p->GridX < 4 || p->GridY < 4 || p->GridX > 32767 || p->GridY > 32767)
+        return icm::fail(ICM_ERR_ARG, "GridX/GridY out of range [4, 32767]");
+    if ((size_t)p->GridX * (size_t)p->GridY > c->cap_nodes)
+        return icm::fail(ICM_ERR_ARG, "GridX*GridY exceeds the allocated grid");
+    if (p->n_indenter_subdivisions < 1 || p->n_indenter_subdivisions > kMaxBins)
+        return icm::fail(ICM_ERR_ARG, "n_indenter_subdivisions out of range [1, 256]");
+    if (!(p->cellsize > 0) || !(p->InitialTimeStep > 0)) return icm::fail(ICM_ERR_ARG, "cellsize/time step not positive");
+    if (p->UpdateEveryNthStep < 1) return icm::fail(ICM_ERR_ARG, "UpdateEveryNthStep < 1");
+    return ICM_OK;
+}
+
+// The kernels' copy of SimParams: the caller's values with this context's
+// device pointers and pitches.
+static icy_SimParams kernel_params(icm_ctx *c, const icy_SimParams *p)
+{
+    icy_SimParams k = *p;
+    k.pts_array = c->d_pts;
+    k.grid_array = c->d_grid;
+    k.indenter_force_accumulator = c->d_bins;
+    k.nPtsPitch = c->pts_pitch;
+    k.nGridPitch = c->grid_pitch;
+    k.GridTotal = p->GridX * p->GridY;
+    return k;
+}
+
+static Consts32 make_consts32(const icy_SimParams &P)
+{
+    Consts32 k;
+    k.h = (float)P.cellsize;
+    k.h_inv = (float)P.cellsize_inv;
+    k.dt = (float)P.InitialTimeStep;
+    k.dt_h_inv = (float)(P.InitialTimeStep * P.cellsize_inv);
+    k.mass = (float)P.ParticleMass;
+    k.stress_c = (float)((P.InitialTimeStep * P.ParticleVolume) * P.Dp_inv);
+    k.mu = (float)P.mu;
+    k.kappa = (float)P.kappa;
+    k.half_kappa = (float)(P.kappa / 2.);
+    k.tan_phi = (float)P.DP_tan_phi;
+    k.p_thr = (float)P.DP_threshold_p;
+    k.pmax_dp = (float)P.IceCompressiveStrength;
+    k.qmax_dp = (float)P.IceShearStrength;
+    double Je_new = std::sqrt(1.0 + 2.0 * P.DP_threshold_p / P.kappa);
+    k.tension_Je_new = (float)Je_new;
+    double a = 2.0 * P.DP_threshold_p / P.kappa;
+    double jm1 = a / (std::sqrt(1.0 + a) + 1.0);
+    k.tension_delta = (float)(jm1 / (std::sqrt(Je_new) + 1.0));
+    k.gv = (float)P.GrainVariability;
+    k.ics = (float)P.IceCompressiveStrength;
+    k.its = (float)P.IceTensileStrength;
+    k.iss = (float)P.IceShearStrength;
+    k.four_h_inv = (float)(4.0 * P.cellsize_inv);
+    return k;
+}
+
+static void free_fused(icm_ctx *c)
+{
+    dfree(c->fz.p64.pos); dfree(c->fz.p64.F); dfree(c->fz.p64.Jp); dfree(c->fz.p64.meta);
+    dfree(c->fz.p64.vel); dfree(c->fz.p64.Bp); dfree(c->fz.p64.pq);
+    dfree(c->fz.p32.cell); dfree(c->fz.p32.frac); dfree(c->fz.p32.H); dfree(c->fz.p32.Jp);
+    dfree(c->fz.p32.meta); dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
+    for (int b = 0; b < 3; b++) { if (c->fz.grid[b]) cudaFree(c->fz.grid[b]); c->fz.grid[b] = nullptr; }
+    dfree(c->fz.dirty);
+    c->fz = Fused{};
+}
+
+static void free_binning(icm_ctx *c)
+{
+    dfree(c->bin.key); dfree(c->bin.count); dfree(c->bin.cell_start); dfree(c->bin.cursor);
+    dfree(c->bin.perm); dfree(c->bin.chunk); dfree(c->bin.tile_start); dfree(c->bin.pid);
+    c->bin = Binning{};
+}
+
+static void geometry(const icy_SimParams &P, int variant, TileGeom &g, int &ntiles)
+{
+    g.TX = kVariants[variant].TX;
+    g.TY = kVariants[variant].TY;
+    g.ntx = (P.GridX + g.TX - 1) / g.TX;
+    g.nty = (P.GridY + g.TY - 1) / g.TY;
+    ntiles = g.ntx * g.nty;
+}
+
+static int ensure_fused(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t ntiles, size_t ncells)
+{
+    if (c->fz.form != form || c->fz.cap_pts < npts || c->fz.cap_nodes < nnodes || c->fz.cap_tiles < ntiles) {
+        free_fused(c);
+        c->fz.form = form;
+        c->fz.cap_pts = npts;
+        c->fz.cap_nodes = nnodes;
+        c->fz.cap_tiles = ntiles;
+        int rc = ICM_OK;
+        if (form == ICM_FORM_FP64) {
+            Parts64 &A = c->fz.p64;
+            if ((rc = dalloc(&A.pos, npts)) || (rc = dalloc(&A.F, npts)) || (rc = dalloc(&A.Jp, npts)) ||
+                (rc = dalloc(&A.meta, npts)) || (rc = dalloc(&A.vel, npts)) || (rc = dalloc(&A.Bp, npts)) ||
+                (rc = dalloc(&A.pq, npts)))
+                return rc;
+            for (int b = 0; b < 3; b++) {
+                Node64 *g;
+                if ((rc = dalloc(&g, nnodes))) return rc;
+                c->fz.grid[b] = g;
+            }
+        } else {
+            Parts32 &A = c->fz.p32;
+            if ((rc = dalloc(&A.cell, npts)) || (rc = dalloc(&A.frac, npts)) || (rc = dalloc(&A.H, npts)) ||
+                (rc = dalloc(&A.Jp, npts)) || (rc = dalloc(&A.meta, npts)) || (rc = dalloc(&A.vel, npts)) ||
+                (rc = dalloc(&A.Bp, npts)) || (rc = dalloc(&A.pq, npts)))
+                return rc;
+            for (int b = 0; b < 3; b++) {
+                float4 *g;
+                if ((rc = dalloc(&g, nnodes))) return rc;
+                c->fz.grid[b] = g;
+            }
+        }
+        if ((rc = dalloc(&c->fz.dirty, 3 * ntiles))) return rc;
+    }
+    if (c->bin.cap_pts < npts || c->bin.cap_cells < ncells || c->bin.cap_tiles < ntiles) {
+        free_binning(c);
+        int rc;
+        size_t nchunks = (ncells + kScanChunk - 1) / kScanChunk;
+        if ((rc = dalloc(&c->bin.key, npts)) || (rc = dalloc(&c->bin.perm, npts)) || (rc = dalloc(&c->bin.pid, npts)) ||
+            (rc = dalloc(&c->bin.count, ncells + 1)) || (rc = dalloc(&c->bin.cell_start, ncells + 1)) ||
+            (rc = dalloc(&c->bin.cursor, ncells + 1)) || (rc = dalloc(&c->bin.chunk, nchunks + 1)) ||
+            (rc = dalloc(&c->bin.tile_start, ntiles + 1)))
+            return rc;
+        c->bin.cap_pts = npts;
+        c->bin.cap_cells = ncells;
+        c->bin.cap_tiles = ntiles;
+    }
+    return ICM_OK;
+}
+
+// Bins the reference SoA by tile and base node and gathers it into the
+// internal arrays of form c->form.
+static int pack(icm_ctx *c, const icy_SimParams &P)
+{
+    TileGeom g;
+    int ntiles;
+    geometry(P, c->tile_variant, g, ntiles);
+    const size_t ncells = (size_t)ntiles * g.TX * g.TY;
+    if (ncells > (size_t)kScanChunk * kScanChunk) return icm::fail(ICM_ERR_ARG, "grid too large for the binning scan");
+    int rc = ensure_fused(c, c->form, (size_t)P.nPts, (size_t)P.GridX * P.GridY, (size_t)ntiles, ncells);
+    if (rc) return rc;
+    cudaStream_t s = c->stream;
+    const int n = P.nPts;
+    const int nchunks = (int)((ncells + kScanChunk - 1) / kScanChunk);
+    ICM_CUDA(cudaMemsetAsync(c->bin.count, 0, sizeof(int) * (ncells + 1), s));
+    if (n > 0) {
+        k_bin_keys<<<(n + 255) / 256, 256, 0, s>>>(P, g, c->bin.key, c->bin.count);
+        ICM_LAUNCHED("k_bin_keys");
+    }
+    k_scan_chunks<<<nchunks, kScanThreads, 0, s>>>(c->bin.count, (int)ncells, c->bin.chunk);
+    ICM_LAUNCHED("k_scan_chunks");
+    k_scan_sums<<<1, kScanThreads, 0, s>>>(c->bin.chunk, nchunks);
+    ICM_LAUNCHED("k_scan_sums");
+    k_scan_apply<<<nchunks, kScanThreads, 0, s>>>(c->bin.count, (int)ncells, c->bin.chunk, c->bin.cell_start);
+    ICM_LAUNCHED("k_scan_apply");
+    ICM_CUDA(cudaMemcpyAsync(c->bin.cursor, c->bin.cell_start, sizeof(int) * ncells, cudaMemcpyDeviceToDevice, s));
+    if (n > 0) {
+        k_bin_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, c->bin.key, c->bin.cursor, c->bin.perm);
+        ICM_LAUNCHED("k_bin_scatter");
+    }
+    k_bin_order<<<(int)((ncells + 255) / 256), 256, 0, s>>>((int)ncells, c->bin.cell_start, c->bin.perm);
+    ICM_LAUNCHED("k_bin_order");
+    k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start);
+    ICM_LAUNCHED("k_tile_starts");
+    if (n > 0) {
+        if (c->form == ICM_FORM_FP64)
+            k_pack64<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.pid, c->fz.p64);
+        else
+            k_pack32<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.pid, c->fz.p32);
+        ICM_LAUNCHED("k_pack");
+    }
+    c->internal_valid = true;
+    c->internal_variant = c->tile_variant;
+    c->internal_pq = false;
+    return ICM_OK;
+}
+
+// Writes the internal state back into the reference SoA if it is current.
+static int ensure_ref(icm_ctx *c)
+{
+    if (c->ref_valid) return ICM_OK;
+    if (!c->internal_valid) return icm::fail(ICM_ERR_STATE, "no valid particle state on the device");
+    const icy_SimParams P = kernel_params(c, &c->prms);
+    const int n = P.nPts;
+    if (n > 0) {
+        if (c->fz.form == ICM_FORM_FP64)
+            k_unpack64<<<(n + 255) / 256, 256, 0, c->stream>>>(P, c->bin.pid, c->fz.p64, c->internal_pq ? 1 : 0);
+        else
+            k_unpack32<<<(n + 255) / 256, 256, 0, c->stream>>>(P, c->bin.pid, c->fz.p32, c->internal_pq ? 1 : 0);
+        ICM_LAUNCHED("k_unpack");
+    }
+    c->ref_valid = true;
+    return ICM_OK;
+}
+
+static int ensure_hist(icm_ctx *c, int n)
+{
+    if ((size_t)n * 2 > c->hist_cap) {
+        dfree(c->d_hist);
+        size_t cap = std::max<size_t>(2 * (size_t)n, 1024);
+        int rc = dalloc(&c->d_hist, cap);
+        if (rc) return rc;
+        c->hist_cap = cap;
+    }
+    return ICM_OK;
+}
+
+// ----------------------------------------------------- fused run dispatch
+
+template <class Pol, int TX, int TY, bool REDUCE>
+static int launch_tile(icm_ctx *c, int mode, int ntiles, const icy_SimParams &P, const typename Pol::Consts &K,
+                       const typename Pol::Parts &A, const TileRun &R)
+{
+    dim3 grid(ntiles), block(c->threads);
+    switch (mode) {
+    case kModeP2GOnly: k_tile_substep<Pol, TX, TY, kModeP2GOnly, REDUCE><<<grid, block, 0, c->stream>>>(P, K, A, R); break;
+    case kModeFull: k_tile_substep<Pol, TX, TY, kModeFull, REDUCE><<<grid, block, 0, c->stream>>>(P, K, A, R); break;
+    default: k_tile_substep<Pol, TX, TY, kModeFinal, REDUCE><<<grid, block, 0, c->stream>>>(P, K, A, R); break;
+    }
+    ICM_LAUNCHED("k_tile_substep");
+    return ICM_OK;
+}
+
+template <class Pol>
+static int launch_variant(icm_ctx *c, int mode, int ntiles, const icy_SimParams &P, const typename Pol::Consts &K,
+                          const typename Pol::Parts &A, const TileRun &R)
+{
+    switch (c->tile_variant) {
+    case 0: return launch_tile<Pol, 16, 8, true>(c, mode, ntiles, P, K, A, R);
+    case 1: return launch_tile<Pol, 16, 16, true>(c, mode, ntiles, P, K, A, R);
+    case 2: return launch_tile<Pol, 32, 8, true>(c, mode, ntiles, P, K, A, R);
+    default: return launch_tile<Pol, 32, 16, true>(c, mode, ntiles, P, K, A, R);
+    }
+}
+
+static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
+{
+    icy_SimParams P = kernel_params(c, p);
+    if (!c->internal_valid || c->fz.form != c->form || c->internal_variant != c->tile_variant) {
+        int rc = ensure_ref(c);
+        if (rc) return rc;
+        if ((rc = pack(c, P))) return rc;
+    }
+    TileGeom g;
+    int ntiles;
+    geometry(P, c->tile_variant, g, ntiles);
+    const size_t nnodes = (size_t)P.GridX * P.GridY;
+    const size_t node_bytes = (c->form == ICM_FORM_FP64) ? sizeof(Node64) : sizeof(float4);
+    cudaStream_t s = c->stream;
+    for (int b = 0; b < 3; b++) ICM_CUDA(cudaMemsetAsync(c->fz.grid[b], 0, node_bytes * nnodes, s));
+    ICM_CUDA(cudaMemsetAsync(c->fz.dirty, 0, 3 * (size_t)ntiles, s));
+    int rc = ensure_hist(c, n);
+    if (rc) return rc;
+    ICM_CUDA(cudaMemsetAsync(c->d_hist, 0, sizeof(double) * 2 * (size_t)n, s));
+    c->hist_n = n;
+
+    TileRun R{};
+    R.ntx = g.ntx;
+    R.nty = g.nty;
+    R.tile_start = c->bin.tile_start;
+    for (int b = 0; b < 3; b++) {
+        R.dirty[b] = c->fz.dirty + (size_t)b * ntiles;
+        R.grid[b] = c->fz.grid[b];
+    }
+    R.bins = c->d_bins;
+    R.err = c->d_err;
+    R.fp64_redo = c->d_redo;
+    R.ind_y = p->indenter_y;
+
+    const Consts32 K32 = make_consts32(P);
+    const Pol64::Consts K64{0};
+    auto launch = [&](int mode) -> int {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (c->ktime && mode == kModeFull) {
+            if (c->kev_used + 2 > c->kev.size()) {
+                for (int k = 0; k < 64; k++) {
+                    cudaEvent_t e;
+                    if (cudaEventCreate(&e) != cudaSuccess) return icm::fail(ICM_ERR_CUDA, "cudaEventCreate");
+                    c->kev.push_back(e);
+                }
+            }
+            e0 = c->kev[c->kev_used++];
+            e1 = c->kev[c->kev_used++];
+            ICM_CUDA(cudaEventRecord(e0, c->stream));
+        }
+        int r = (c->form == ICM_FORM_FP64) ? launch_variant<Pol64>(c, mode, ntiles, P, K64, c->fz.p64, R)
+                                           : launch_variant<Pol32>(c, mode, ntiles, P, K32, c->fz.p32, R);
+        if (e1) ICM_CUDA(cudaEventRecord(e1, c->stream));
+        return r;
+    };
+    // prologue: P2G of the current state into G[0]
+    R.bufA = 0; R.bufB = 0; R.bufC = 0;
+    R.force_slot = nullptr;
+    R.record_pq = 0;
+    R.ind_x = p->indenter_x;
+    if ((rc = launch(kModeP2GOnly))) return rc;
+    double t = p->SimulationTime;
+    bool any_pq = false;
+    for (int k = 1; k <= n; k++) {
+        t += p->InitialTimeStep;
+        p->indenter_x = p->indenter_x_initial + t * p->IndVelocity;
+        const int sidx = k - 1;
+        R.bufA = sidx % 3;
+        R.bufB = (sidx + 1) % 3;
+        R.bufC = (sidx + 2) % 3;
+        R.ind_x = p->indenter_x;
+        R.force_slot = c->d_hist + 2 * (size_t)sidx;
+        R.record_pq = ((p->SimulationStep + k) % p->UpdateEveryNthStep == 0) ? 1 : 0;
+        any_pq |= R.record_pq != 0;
+        if ((rc = launch(k < n ? kModeFull : kModeFinal))) return rc;
+    }
+    p->SimulationStep += n;
+    p->SimulationTime = t;
+    c->internal_valid = true;
+    c->ref_valid = false;
+    c->internal_pq = c->internal_pq || any_pq;
+    return ICM_OK;
+}
+
+static int run_stepwise(icm_ctx *c, icy_SimParams *p, int n)
+{
+    int rc = ensure_ref(c);
+    if (rc) return rc;
+    if ((rc = ensure_hist(c, n))) return rc;
+    cudaStream_t s = c->stream;
+    ICM_CUDA(cudaMemsetAsync(c->d_hist, 0, sizeof(double) * 2 * (size_t)n, s));
+    c->hist_n = n;
+    double t = p->SimulationTime;
+    for (int k = 1; k <= n; k++) {
+        t += p->InitialTimeStep;
+        p->indenter_x = p->indenter_x_initial + t * p->IndVelocity;
+        icy_SimParams P = kernel_params(c, p);
+        ICM_CUDA(cudaMemsetAsync(c->d_grid, 0, sizeof(double) * c->grid_pitch * ICM_N_GRID_ARRAYS, s));
+        const int tp = P.tpb_P2G > 0 ? P.tpb_P2G : 256, tu = P.tpb_Upd > 0 ? P.tpb_Upd : 512;
+        const int tg = P.tpb_G2P > 0 ? P.tpb_G2P : 128;
+        if (P.nPts > 0) {
+            k_p2g_ref64<<<(P.nPts + tp - 1) / tp, tp, 0, s>>>(P, c->d_err);
+            ICM_LAUNCHED("cuda_p2g");
+        }
+        k_update_ref64<<<(P.GridTotal + tu - 1) / tu, tu, 0, s>>>(P, p->indenter_x, p->indenter_y,
+                                                                  c->d_hist + 2 * (size_t)(k - 1));
+        ICM_LAUNCHED("cuda_update_nodes");
+        if (P.nPts > 0) {
+            k_g2p_ref64<<<(P.nPts + tg - 1) / tg, tg, 0, s>>>(P, (p->SimulationStep + k) % p->UpdateEveryNthStep == 0);
+            ICM_LAUNCHED("cuda_g2p");
+        }
+    }
+    p->SimulationStep += n;
+    p->SimulationTime = t;
+    c->internal_valid = false;
+    c->ref_valid = true;
+    return ICM_OK;
+}
+
+// ------------------------------------------------------------------- ABI
+
+extern "C" int icm_create(icm_ctx **out, int device)
+{
+    if (!out) return icm::fail(ICM_ERR_ARG, "icm_create: null out");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return icm::fail(ICM_ERR_NODEVICE, std::string("No avaialble CUDA devices: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= count) return icm::fail(ICM_ERR_ARG, "icm_create: device index out of range");
+    ICM_CUDA(cudaSetDevice(device));
+    icm_ctx *c = new icm_ctx();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev_start) != cudaSuccess || cudaEventCreate(&c->ev_stop) != cudaSuccess ||
+        cudaMalloc((void **)&c->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void **)&c->d_redo, sizeof(unsigned long long)) != cudaSuccess) {
+        icm_destroy(c);
+        return icm::fail(ICM_ERR_CUDA, "icm_create: stream/event/allocation failed");
+    }
+    cudaMemset(c->d_err, 0, sizeof(int));
+    cudaMemset(c->d_redo, 0, sizeof(unsigned long long));
+    *out = c;
+    return ICM_OK;
+}
+
+extern "C" int icm_destroy(icm_ctx *c)
+{
+    if (!c) return ICM_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_fused(c);
+    free_binning(c);
+    dfree(c->d_pts); dfree(c->d_grid); dfree(c->d_bins); dfree(c->d_err); dfree(c->d_hist); dfree(c->d_redo);
+    for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
+    if (c->ev_start) cudaEventDestroy(c->ev_start);
+    if (c->ev_stop) cudaEventDestroy(c->ev_stop);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return ICM_OK;
+}
+
+extern "C" int icm_set_form(icm_ctx *c, int form)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    if (form < ICM_FORM_FP64_STEPWISE || form > ICM_FORM_FP32) return icm::fail(ICM_ERR_ARG, "unknown form");
+    if (form == c->form) return ICM_OK;
+    if (c->d_pts) {
+        int rc = ensure_ref(c);
+        if (rc) return rc;
+    }
+    c->internal_valid = false;
+    c->form = form;
+    return ICM_OK;
+}
+
+extern "C" int icm_get_form(icm_ctx *c) { return c ? c->form : -1; }
+
+extern "C" int icm_set_tile(icm_ctx *c, int variant, int threads)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    if (variant < 0 || variant > 3) return icm::fail(ICM_ERR_ARG, "tile variant must be 0..3");
+    if (threads < 32 || threads > 256 || threads % 32) return icm::fail(ICM_ERR_ARG, "threads must be 32..256, multiple of 32");
+    if (variant != c->tile_variant && c->d_pts) {
+        int rc = ensure_ref(c);
+        if (rc) return rc;
+        c->internal_valid = false;
+    }
+    c->tile_variant = variant;
+    c->threads = threads;
+    return ICM_OK;
+}
+
+extern "C" int icm_get_tile(icm_ctx *c, int *variant, int *threads)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    if (variant) *variant = c->tile_variant;
+    if (threads) *threads = c->threads;
+    return ICM_OK;
+}
+
+extern "C" int icm_allocate_arrays(icm_ctx *c, icy_SimParams *p, size_t n_grid_nodes, size_t n_points)
+{
+    if (!c || !p) return icm::fail(ICM_ERR_ARG, "null argument");
+    if (n_points > 0x7fffffffULL || n_grid_nodes > 0x7fffffffULL) return icm::fail(ICM_ERR_ARG, "sizes too large");
+    ICM_CUDA(cudaSetDevice(c->device));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    dfree(c->d_pts);
+    dfree(c->d_grid);
+    dfree(c->d_bins);
+    free_fused(c);
+    free_binning(c);
+    c->pts_pitch = icm_pitch_elems(n_points);
+    c->grid_pitch = icm_pitch_elems(n_grid_nodes);
+    int rc;
+    if ((rc = dalloc(&c->d_pts, c->pts_pitch * ICM_N_PTS_ARRAYS))) return rc;
+    if ((rc = dalloc(&c->d_grid, c->grid_pitch * ICM_N_GRID_ARRAYS))) return rc;
+    if ((rc = dalloc(&c->d_bins, (size_t)2 * kMaxBins))) return rc;
+    ICM_CUDA(cudaMemset(c->d_pts, 0, sizeof(double) * c->pts_pitch * ICM_N_PTS_ARRAYS));
+    ICM_CUDA(cudaMemset(c->d_grid, 0, sizeof(double) * c->grid_pitch * ICM_N_GRID_ARRAYS));
+    ICM_CUDA(cudaMemset(c->d_bins, 0, sizeof(double) * 2 * kMaxBins));
+    ICM_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+    c->cap_pts = n_points;
+    c->cap_nodes = n_grid_nodes;
+    p->pts_array = c->d_pts;
+    p->grid_array = c->d_grid;
+    p->indenter_force_accumulator = c->d_bins;
+    p->nPtsPitch = c->pts_pitch;
+    p->nGridPitch = c->grid_pitch;
+    c->prms = *p;
+    c->ref_valid = true;
+    c->internal_valid = false;
+    return ICM_OK;
+}
+
+extern "C" int icm_update_constants(icm_ctx *c, const icy_SimParams *p, int error_code)
+{
+    if (!c || !p) return icm::fail(ICM_ERR_ARG, "null argument");
+    int rc = check_params(c, p);
+    if (rc) return rc;
+    ICM_CUDA(cudaMemcpyAsync(c->d_err, &error_code, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    c->prms = *p;
+    return ICM_OK;
+}
+
+extern "C" int icm_transfer_points_to_device(icm_ctx *c, const double *host_soa)
+{
+    if (!c || !host_soa) return icm::fail(ICM_ERR_ARG, "null argument");
+    if (!c->d_pts) return icm::fail(ICM_ERR_STATE, "arrays are not allocated");
+    ICM_CUDA(cudaMemcpyAsync(c->d_pts, host_soa, sizeof(double) * c->pts_pitch * ICM_N_PTS_ARRAYS,
+                             cudaMemcpyHostToDevice, c->stream));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    c->ref_valid = true;
+    c->internal_valid = false;
+    return ICM_OK;
+}
+
+extern "C" int icm_reset_grid(icm_ctx *c)
+{
+    if (!c || !c->d_grid) return icm::fail(ICM_ERR_STATE, "arrays are not allocated");
+    ICM_CUDA(cudaMemsetAsync(c->d_grid, 0, sizeof(double) * c->grid_pitch * ICM_N_GRID_ARRAYS, c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_reset_indenter_force_accumulator(icm_ctx *c)
+{
+    if (!c || !c->d_bins) return icm::fail(ICM_ERR_STATE, "arrays are not allocated");
+    ICM_CUDA(cudaMemsetAsync(c->d_bins, 0, sizeof(double) * 2 * kMaxBins, c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_p2g(icm_ctx *c)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    int rc = check_params(c, &c->prms);
+    if (rc || (rc = ensure_ref(c))) return rc;
+    icy_SimParams P = kernel_params(c, &c->prms);
+    int tpb = P.tpb_P2G > 0 ? P.tpb_P2G : 256;
+    if (P.nPts > 0) {
+        k_p2g_ref64<<<(P.nPts + tpb - 1) / tpb, tpb, 0, c->stream>>>(P, c->d_err);
+        ICM_LAUNCHED("cuda_p2g");
+    }
+    return ICM_OK;
+}
+
+extern "C" int icm_update_nodes(icm_ctx *c, double indenter_x, double indenter_y)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    int rc = check_params(c, &c->prms);
+    if (rc) return rc;
+    icy_SimParams P = kernel_params(c, &c->prms);
+    int tpb = P.tpb_Upd > 0 ? P.tpb_Upd : 512;
+    k_update_ref64<<<(P.GridTotal + tpb - 1) / tpb, tpb, 0, c->stream>>>(P, indenter_x, indenter_y, nullptr);
+    ICM_LAUNCHED("cuda_update_nodes");
+    return ICM_OK;
+}
+
+extern "C" int icm_g2p(icm_ctx *c, int record_pq)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    int rc = check_params(c, &c->prms);
+    if (rc || (rc = ensure_ref(c))) return rc;
+    icy_SimParams P = kernel_params(c, &c->prms);
+    int tpb = P.tpb_G2P > 0 ? P.tpb_G2P : 128;
+    if (P.nPts > 0) {
+        k_g2p_ref64<<<(P.nPts + tpb - 1) / tpb, tpb, 0, c->stream>>>(P, record_pq ? 1 : 0);
+        ICM_LAUNCHED("cuda_g2p");
+    }
+    c->internal_valid = false;
+    return ICM_OK;
+}
+
+extern "C" int icm_transfer_from_device(icm_ctx *c, double *host_soa, double *host_bins, int *error_code,
+                                        icm_host_fn cb, void *user)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    if (!c->d_pts) return icm::fail(ICM_ERR_STATE, "arrays are not allocated");
+    int rc = ensure_ref(c);
+    if (rc) return rc;
+    cudaStream_t s = c->stream;
+    if (host_soa)
+        ICM_CUDA(cudaMemcpyAsync(host_soa, c->d_pts, sizeof(double) * c->pts_pitch * ICM_N_PTS_ARRAYS,
+                                 cudaMemcpyDeviceToHost, s));
+    if (host_bins)
+        ICM_CUDA(cudaMemcpyAsync(host_bins, c->d_bins, sizeof(double) * 2 * c->prms.n_indenter_subdivisions,
+                                 cudaMemcpyDeviceToHost, s));
+    if (error_code) ICM_CUDA(cudaMemcpyAsync(error_code, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (cb) ICM_CUDA(cudaLaunchHostFunc(s, (cudaHostFn_t)cb, user));
+    return ICM_OK;
+}
+
+extern "C" int icm_transfer_grid_to_device(icm_ctx *c, const double *host_grid)
+{
+    if (!c || !host_grid) return icm::fail(ICM_ERR_ARG, "null argument");
+    if (!c->d_grid) return icm::fail(ICM_ERR_STATE, "arrays are not allocated");
+    ICM_CUDA(cudaMemcpyAsync(c->d_grid, host_grid, sizeof(double) * c->grid_pitch * ICM_N_GRID_ARRAYS,
+                             cudaMemcpyHostToDevice, c->stream));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_transfer_grid_from_device(icm_ctx *c, double *host_grid)
+{
+    if (!c || !host_grid) return icm::fail(ICM_ERR_ARG, "null argument");
+    if (!c->d_grid) return icm::fail(ICM_ERR_STATE, "arrays are not allocated");
+    ICM_CUDA(cudaMemcpyAsync(host_grid, c->d_grid, sizeof(double) * c->grid_pitch * ICM_N_GRID_ARRAYS,
+                             cudaMemcpyDeviceToHost, c->stream));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_synchronize(icm_ctx *c)
+{
+    if (!c) return ICM_OK;
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_run_substeps(icm_ctx *c, icy_SimParams *p, int n)
+{
+    if (!c || !p) return icm::fail(ICM_ERR_ARG, "null argument");
+    if (n < 0) return icm::fail(ICM_ERR_ARG, "negative substep count");
+    int rc = check_params(c, p);
+    if (rc) return rc;
+    c->prms = *p;
+    if (n == 0) return ICM_OK;
+    rc = (c->form == ICM_FORM_FP64_STEPWISE) ? run_stepwise(c, p, n) : run_fused(c, p, n);
+    c->prms = *p;
+    return rc;
+}
+
+extern "C" int icm_force_history(icm_ctx *c, double *host_out, int n)
+{
+    if (!c || !host_out) return icm::fail(ICM_ERR_ARG, "null argument");
+    if (n < 0 || n > c->hist_n) return icm::fail(ICM_ERR_ARG, "history shorter than requested");
+    if (n == 0) return ICM_OK;
+    ICM_CUDA(cudaMemcpyAsync(host_out, c->d_hist, sizeof(double) * 2 * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_fp64_redo_count(icm_ctx *c, unsigned long long *out)
+{
+    if (!c || !out) return icm::fail(ICM_ERR_ARG, "null argument");
+    ICM_CUDA(cudaMemcpyAsync(out, c->d_redo, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_record_start(icm_ctx *c)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    ICM_CUDA(cudaEventRecord(c->ev_start, c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_record_stop(icm_ctx *c)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    ICM_CUDA(cudaEventRecord(c->ev_stop, c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_elapsed_ms(icm_ctx *c, float *ms)
+{
+    if (!c || !ms) return icm::fail(ICM_ERR_ARG, "null argument");
+    ICM_CUDA(cudaEventSynchronize(c->ev_stop));
+    ICM_CUDA(cudaEventElapsedTime(ms, c->ev_start, c->ev_stop));
+    return ICM_OK;
+}
+
+// Accumulates the recorded launch pairs into ktime_ms (synchronises).
+static int harvest_ktime(icm_ctx *c)
+{
+    if (c->kev_used == 0) return ICM_OK;
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    for (size_t k = 0; k + 1 < c->kev_used; k += 2) {
+        float ms = 0;
+        ICM_CUDA(cudaEventElapsedTime(&ms, c->kev[k], c->kev[k + 1]));
+        c->ktime_ms += ms;
+        c->ktime_count++;
+    }
+    c->kev_used = 0;
+    return ICM_OK;
+}
+
+extern "C" int icm_kernel_timing(icm_ctx *c, int enable)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    int rc = harvest_ktime(c);
+    if (rc) return rc;
+    c->ktime = enable != 0;
+    c->ktime_ms = 0;
+    c->ktime_count = 0;
+    return ICM_OK;
+}
+
+extern "C" int icm_kernel_time(icm_ctx *c, double *total_ms, long long *launches)
+{
+    if (!c || !total_ms || !launches) return icm::fail(ICM_ERR_ARG, "null argument");
+    int rc = harvest_ktime(c);
+    if (rc) return rc;
+    *total_ms = c->ktime_ms;
+    *launches = c->ktime_count;
+    return ICM_OK;
+}
+
+extern "C" void *icm_stream(icm_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+extern "C" int icm_host_alloc(void **ptr, size_t bytes)
+{
+    if (!ptr) return icm::fail(ICM_ERR_ARG, "null argument");
+    ICM_CUDA(cudaMallocHost(ptr, bytes));
+    return ICM_OK;
+}
+
+extern "C" int icm_host_free(void *ptr)
+{
+    if (ptr) ICM_CUDA(cudaFreeHost(ptr));
+    return ICM_OK;
+}

@@ -1,0 +1,800 @@
+// k_tiles.cuh -- the fused substep: grid update + G2P + P2G in ONE launch.
+//
+// Data layout in HBM (internal, "tile order"):
+//   * particles are binned by the node tile (TX x TY grid nodes) that holds
+//     their stencil base node (int)(x/h - 0.5) and, inside a tile, sorted by
+//     base node; every array is a dense structure-of-arrays in that order, so
+//     a warp reads 32 consecutive particles with one vector load per field;
+//   * the grid is three full-size node buffers G[0..2] of {m, px, py, -};
+//     substep s reads G[s%3] (P2G result of substep s-1), scatters into
+//     G[(s+1)%3] and zeroes G[(s+2)%3] (read by substep s-1), so no separate
+//     reset or update launch is needed;
+//   * dirty[b][t] flags tile t of buffer b as possibly non-zero.
+//
+// One CTA owns one node tile t and its particles:
+//   1. zero t's nodes in G[(s+2)%3] if dirty;
+//   2. grid update (v2_kernel_update_nodes, gpu_implementation5.cu:215-290)
+//      of the (TX+4) x (TY+4) node region around t into shared memory: the
+//      region is every node a particle of t can reach after drifting up to
+//      one node from its tile. Halo nodes are recomputed by neighbouring CTAs
+//      (the update is a pure function of the node); only the owner of a node
+//      adds its reaction force, reduced in shared memory in FP64;
+//   3. per particle G2P (v2_kernel_g2p, :294-379) from the shared velocities,
+//      advection, Fe update, constitutive model, store;
+//   4. P2G (v2_kernel_p2g, :148-213) of the updated particle for substep s+1
+//      into a shared accumulation region, with a segmented warp-shuffle
+//      reduction over lanes that share a base node before the shared
+//      atomics; particles whose stencil leaves the region fall back to global
+//      atomics;
+//   5. the shared region is added to G[(s+1)%3] with one vector atomic per
+//      touched node (red.global.add.v4.f32 in FP32) and the touched tiles are
+//      flagged dirty.
+// Velocity v and affine matrix Bp never leave registers between substeps;
+// they are written only by the final launch of a run.
+#pragma once
+#include <cstdint>
+#include "mpm_math32.cuh"
+
+namespace icm {
+
+enum { kModeP2GOnly = 0, kModeFull = 1, kModeFinal = 2 };
+constexpr int kMaxBins = 256;
+
+struct alignas(16) Node64 { double m, px, py, pad; };
+
+struct TileRun {
+    int ntx, nty;
+    const int *tile_start;   // ntiles + 1
+    uint8_t *dirty[3];       // ntiles flags per buffer
+    void *grid[3];
+    int bufA, bufB, bufC;    // read / scatter / zero
+    double ind_x, ind_y;
+    double *bins;            // 2*n_indenter_subdivisions, accumulated
+    double *force_slot;      // 2 doubles: this substep's summed reaction
+    int *err;
+    int record_pq;
+    unsigned long long *fp64_redo;
+};
+
+struct Parts64 { double2 *pos; double4 *F; double *Jp; uint32_t *meta; double2 *vel; double4 *Bp; double2 *pq; };
+struct Parts32 { uint32_t *cell; float2 *frac; float4 *H; float *Jp; uint32_t *meta; float2 *vel; float4 *Bp; float2 *pq; };
+
+__device__ __forceinline__ uint32_t pack_cell(int ix, int iy) { return (uint32_t)(uint16_t)(int16_t)ix | ((uint32_t)(uint16_t)(int16_t)iy << 16); }
+__device__ __forceinline__ int cell_x(uint32_t c) { return (int)(int16_t)(uint16_t)(c & 0xffffu); }
+__device__ __forceinline__ int cell_y(uint32_t c) { return (int)(int16_t)(uint16_t)(c >> 16); }
+
+// ---------------------------------------------------------------- policies
+
+// FP64 reference form: absolute positions, Fe, Jp_inv in double.
+struct Pol64 {
+    using real = double;
+    using Node = Node64;
+    using Parts = Parts64;
+    struct Consts { int dummy; };
+    struct St { double x, y; M2d F; double Jp; uint32_t meta; };
+    struct Sten { int bx, by; double fx, fy, wx[3], wy[3]; };
+
+    static __device__ __forceinline__ Sten stencil(const icy_SimParams &P, const Consts &, const St &s)
+    {
+        Stencil64 t = stencil64(s.x, s.y, P.cellsize_inv);
+        Sten r;
+        r.bx = t.bx; r.by = t.by; r.fx = t.fx; r.fy = t.fy;
+#pragma unroll
+        for (int i = 0; i < 3; i++) { r.wx[i] = t.wx[i]; r.wy[i] = t.wy[i]; }
+        return r;
+    }
+    static __device__ __forceinline__ St load(const Parts &A, int p)
+    {
+        St s;
+        double2 x = A.pos[p];
+        double4 F = A.F[p];
+        s.x = x.x; s.y = x.y;
+        s.F = {F.x, F.y, F.z, F.w};
+        s.Jp = A.Jp[p];
+        s.meta = A.meta[p];
+        return s;
+    }
+    static __device__ __forceinline__ void node_velocity(const icy_SimParams &P, const Consts &, const Node &n, int gx,
+                                                         int gy, double ix, double iy, double &v0, double &v1,
+                                                         double &f0, double &f1, int &bin)
+    {
+        bin = -1;
+        if (n.m == 0) { v0 = 0; v1 = 0; return; }
+        NodeOut o = update_node64(P, gx, gy, n.m, n.px, n.py, ix, iy);
+        v0 = o.v0; v1 = o.v1; f0 = o.f0; f1 = o.f1; bin = o.bin;
+    }
+    // G2P tail: advect, Fe update, constitutive model.
+    static __device__ __forceinline__ void advance(const icy_SimParams &P, const Consts &, St &s, double v0, double v1,
+                                                   const double B[4], double &p_tr, double &q_tr, int &redo)
+    {
+        const double dt = P.InitialTimeStep;
+        s.x += v0 * dt;
+        s.y += v1 * dt;
+        double M00 = 1 + dt * B[0], M01 = dt * B[1], M10 = dt * B[2], M11 = 1 + dt * B[3];
+        M2d F = s.F;
+        s.F = {M00 * F.a00 + M01 * F.a10, M00 * F.a01 + M01 * F.a11, M10 * F.a00 + M11 * F.a10, M10 * F.a01 + M11 * F.a11};
+        uint8_t cr = (uint8_t)(s.meta >> 16);
+        constitutive64(P, s.F, s.Jp, cr, (int)(int16_t)(s.meta & 0xffffu), p_tr, q_tr);
+        s.meta = (s.meta & 0xffffu) | ((uint32_t)cr << 16);
+        redo = 0;
+    }
+    static __device__ __forceinline__ void store(const Parts &A, int p, const St &s, const St &old)
+    {
+        A.pos[p] = make_double2(s.x, s.y);
+        A.F[p] = make_double4(s.F.a00, s.F.a01, s.F.a10, s.F.a11);
+        if (s.Jp != old.Jp) A.Jp[p] = s.Jp;
+        if (s.meta != old.meta) A.meta[p] = s.meta;
+    }
+    // stress impulse of P2G: S = m Bp - dt Vp Dinv tau
+    static __device__ __forceinline__ void p2g_matrix(const icy_SimParams &P, const Consts &, const St &s, const double B[4],
+                                                      double S[4])
+    {
+        M2d tau = kirchhoff64(s.F, P.mu, P.kappa);
+        const double m = P.ParticleMass;
+        double c = (P.InitialTimeStep * P.ParticleVolume) * P.Dp_inv;
+        S[0] = m * B[0] - c * tau.a00;
+        S[1] = m * B[1] - c * tau.a01;
+        S[2] = m * B[2] - c * tau.a10;
+        S[3] = m * B[3] - c * tau.a11;
+    }
+    static __device__ __forceinline__ double mass(const icy_SimParams &P, const Consts &) { return P.ParticleMass; }
+    static __device__ __forceinline__ double h(const icy_SimParams &P, const Consts &) { return P.cellsize; }
+    static __device__ __forceinline__ double four_h_inv(const icy_SimParams &P, const Consts &) { return 4. * P.cellsize_inv; }
+};
+
+// FP32 strain form: position = int16 cell + FP32 fraction, H = Fe - I.
+struct Pol32 {
+    using real = float;
+    using Node = float4;
+    using Parts = Parts32;
+    using Consts = Consts32;
+    struct St { int ix, iy; float fx, fy; M2f H; float Jp; uint32_t meta; };
+    struct Sten { int bx, by; float fx, fy, wx[3], wy[3]; };
+
+    static __device__ __forceinline__ void base_of(int ic, float f, int &b, float &fr)
+    {
+        // reference: b = (int)(X - 0.5) (truncation), fr = X - b
+        if (ic >= 1 || (ic == 0 && f >= 0.5f)) {
+            if (f >= 0.5f) { b = ic; fr = f; }
+            else { b = ic - 1; fr = f + 1.0f; }
+        } else {
+            float X = (float)ic + f;
+            b = (int)(X - 0.5f);
+            fr = X - (float)b;
+        }
+    }
+    static __device__ __forceinline__ Sten stencil(const icy_SimParams &, const Consts &, const St &s)
+    {
+        Sten r;
+        base_of(s.ix, s.fx, r.bx, r.fx);
+        base_of(s.iy, s.fy, r.by, r.fy);
+        float a0 = 1.5f - r.fx, a1 = r.fx - 1.0f, a2 = r.fx - 0.5f;
+        r.wx[0] = 0.5f * a0 * a0; r.wx[1] = 0.75f - a1 * a1; r.wx[2] = 0.5f * a2 * a2;
+        float b0 = 1.5f - r.fy, b1 = r.fy - 1.0f, b2 = r.fy - 0.5f;
+        r.wy[0] = 0.5f * b0 * b0; r.wy[1] = 0.75f - b1 * b1; r.wy[2] = 0.5f * b2 * b2;
+        return r;
+    }
+    static __device__ __forceinline__ St load(const Parts &A, int p)
+    {
+        St s;
+        uint32_t c = A.cell[p];
+        float2 f = A.frac[p];
+        float4 H = A.H[p];
+        s.ix = cell_x(c); s.iy = cell_y(c);
+        s.fx = f.x; s.fy = f.y;
+        s.H = {H.x, H.y, H.z, H.w};
+        s.Jp = A.Jp[p];
+        s.meta = A.meta[p];
+        return s;
+    }
+    static __device__ __forceinline__ void node_velocity(const icy_SimParams &P, const Consts &k, const Node &n, int gx,
+                                                         int gy, double ind_x, double ind_y, float &v0, float &v1,
+                                                         double &f0, double &f1, int &bin)
+    {
+        bin = -1;
+        if (n.x == 0.0f) { v0 = 0.0f; v1 = 0.0f; return; }
+        float a = n.y / n.x, b = n.z / n.x;
+        b -= k.dt * (float)P.Gravity;
+        float vmax = 0.5f * k.h / k.dt;
+        float nrm = sqrtf(a * a + b * b);
+        if (nrm > vmax) { a = a / nrm * vmax; b = b / nrm * vmax; }
+        // contact geometry and reaction in FP64
+        double n0 = gx * P.cellsize - ind_x, n1 = gy * P.cellsize - ind_y;
+        if (n0 * n0 + n1 * n1 < P.IndRSq) {
+            const double vco0 = P.IndVelocity;
+            double va = a, vb = b;
+            double vr0 = va - vco0, vr1 = vb;
+            double z = n0 * n0 + n1 * n1;
+            if (z > 0) { double nn = sqrt(z); n0 /= nn; n1 /= nn; }
+            double vn = vr0 * n0 + vr1 * n1;
+            if (vn < 0) {
+                double vt0 = vr0 - n0 * vn, vt1 = vr1 - n1 * vn;
+                double w0 = vco0 + vt0, w1 = vt1;
+                double mass = n.x;
+                f0 = (va - w0) * mass / P.InitialTimeStep;
+                f1 = (vb - w1) * mass / P.InitialTimeStep;
+                double angle = atan2(n0, n1) + ICM_PI;
+                angle *= P.n_indenter_subdivisions / (2 * ICM_PI);
+                int index = (int)angle;
+                index = max(index, 0);
+                index = min(index, P.n_indenter_subdivisions - 1);
+                bin = index;
+                a = (float)w0;
+                b = (float)w1;
+            }
+        }
+        if (gy <= 2) { a = 0.0f; b = 0.0f; }
+        else if (gy >= P.GridY - 3 && b > 0.0f) b = 0.0f;
+        if (gx <= 2 && a < 0.0f) a = 0.0f;
+        else if (gx >= P.GridX - 3 && a > 0.0f) a = 0.0f;
+        v0 = a; v1 = b;
+    }
+    static __device__ __forceinline__ void advance(const icy_SimParams &P, const Consts &k, St &s, float v0, float v1,
+                                                   const float B[4], float &p_tr, float &q_tr, int &redo)
+    {
+        // position: fraction inside the cell, renormalised to [0, 1)
+        float fx = s.fx + v0 * k.dt_h_inv, fy = s.fy + v1 * k.dt_h_inv;
+        float flx = floorf(fx), fly = floorf(fy);
+        s.ix += (int)flx; s.iy += (int)fly;
+        fx -= flx; fy -= fly;
+        if (fx >= 1.0f) { fx -= 1.0f; s.ix += 1; }
+        if (fy >= 1.0f) { fy -= 1.0f; s.iy += 1; }
+        s.fx = fx; s.fy = fy;
+        // H_new = H + dt (C + C H)
+        float c00 = k.dt * B[0], c01 = k.dt * B[1], c10 = k.dt * B[2], c11 = k.dt * B[3];
+        M2f H = s.H;
+        s.H.a00 = H.a00 + (c00 + (c00 * H.a00 + c01 * H.a10));
+        s.H.a01 = H.a01 + (c01 + (c00 * H.a01 + c01 * H.a11));
+        s.H.a10 = H.a10 + (c10 + (c10 * H.a00 + c11 * H.a10));
+        s.H.a11 = H.a11 + (c11 + (c10 * H.a01 + c11 * H.a11));
+        uint8_t cr = (uint8_t)(s.meta >> 16);
+        int grain = (int)(int16_t)(s.meta & 0xffffu);
+        redo = 0;
+        if (constitutive32(k, s.H, s.Jp, cr, grain, p_tr, q_tr) == kC32_NEEDS_FP64) {
+            constitutive32_via64(P, s.H, s.Jp, cr, grain, p_tr, q_tr);
+            redo = 1;
+        }
+        s.meta = (s.meta & 0xffffu) | ((uint32_t)cr << 16);
+    }
+    static __device__ __forceinline__ void store(const Parts &A, int p, const St &s, const St &old)
+    {
+        A.cell[p] = pack_cell(s.ix, s.iy);
+        A.frac[p] = make_float2(s.fx, s.fy);
+        A.H[p] = make_float4(s.H.a00, s.H.a01, s.H.a10, s.H.a11);
+        if (s.Jp != old.Jp) A.Jp[p] = s.Jp;
+        if (s.meta != old.meta) A.meta[p] = s.meta;
+    }
+    static __device__ __forceinline__ void p2g_matrix(const icy_SimParams &, const Consts &k, const St &s, const float B[4],
+                                                      float S[4])
+    {
+        M2f tau = kirchhoff32(s.H, k.mu, k.kappa);
+        S[0] = k.mass * B[0] - k.stress_c * tau.a00;
+        S[1] = k.mass * B[1] - k.stress_c * tau.a01;
+        S[2] = k.mass * B[2] - k.stress_c * tau.a10;
+        S[3] = k.mass * B[3] - k.stress_c * tau.a11;
+    }
+    static __device__ __forceinline__ float mass(const icy_SimParams &, const Consts &k) { return k.mass; }
+    static __device__ __forceinline__ float h(const icy_SimParams &, const Consts &k) { return k.h; }
+    static __device__ __forceinline__ float four_h_inv(const icy_SimParams &, const Consts &k) { return k.four_h_inv; }
+};
+
+// ------------------------------------------------------- grid node access
+
+__device__ __forceinline__ void node_zero(Node64 *g, size_t i) { g[i] = Node64{0, 0, 0, 0}; }
+__device__ __forceinline__ void node_zero(float4 *g, size_t i) { g[i] = make_float4(0.f, 0.f, 0.f, 0.f); }
+
+__device__ __forceinline__ void node_add_global(Node64 *g, size_t i, double m, double px, double py)
+{
+    atomicAdd(&g[i].m, m);
+    atomicAdd(&g[i].px, px);
+    atomicAdd(&g[i].py, py);
+}
+__device__ __forceinline__ void node_add_global(float4 *g, size_t i, float m, float px, float py)
+{
+    atomicAdd(&g[i], make_float4(m, px, py, 0.0f));  // red.global.add.v4.f32 (sm_90+)
+}
+
+// ---------------------------------------------------- warp pre-reduction
+
+// Sums a, b, c over runs of consecutive lanes with equal key; the first lane
+// of each run ends up holding the run's totals. Returns true for run heads.
+template <int N, class T>
+__device__ __forceinline__ bool warp_segment_sum(int key, T (&a)[N], T (&b)[N], T (&c)[N])
+{
+    const unsigned FULL = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+    int prev = __shfl_up_sync(FULL, key, 1);
+    bool head = (lane == 0) || (prev != key);
+    unsigned heads = __ballot_sync(FULL, head);
+    unsigned above = (lane == 31) ? 0u : (heads & (0xffffffffu << (lane + 1)));
+    int seg_end = above ? (__ffs(above) - 1) : 32;
+    int len = head ? (seg_end - lane) : 0;
+    int maxlen = __reduce_max_sync(FULL, len);
+    for (int o = 1; o < maxlen; o <<= 1) {
+        bool take = (lane + o) < seg_end;
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            T oa = __shfl_down_sync(FULL, a[k], o);
+            T ob = __shfl_down_sync(FULL, b[k], o);
+            T oc = __shfl_down_sync(FULL, c[k], o);
+            if (take) { a[k] += oa; b[k] += ob; c[k] += oc; }
+        }
+    }
+    return head;
+}
+
+// ------------------------------------------------------------ the kernel
+
+template <class Pol, int TX, int TY, int MODE, bool REDUCE>
+__global__ void __launch_bounds__(256) k_tile_substep(const icy_SimParams P, const typename Pol::Consts K,
+                                                      const typename Pol::Parts A, const TileRun R)
+{
+    using real = typename Pol::real;
+    using Node = typename Pol::Node;
+    constexpr int RX = TX + 4, RY = TY + 4, RN = RX * RY;
+    __shared__ real s_v0[RN], s_v1[RN];
+    __shared__ real s_am[RN], s_ax[RN], s_ay[RN];
+    __shared__ double s_bins[2 * kMaxBins];
+    __shared__ double s_tot[2];
+    __shared__ int s_contact, s_mark[9];
+
+    const int t = blockIdx.x;
+    const int tx = t % R.ntx, ty = t / R.ntx;
+    const int x0 = tx * TX, y0 = ty * TY;
+    const int rx0 = x0 - 1, ry0 = y0 - 1;
+    const int GX = P.GridX, GY = P.GridY;
+    const int p0 = R.tile_start[t], p1 = R.tile_start[t + 1];
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    Node *gA = (Node *)R.grid[R.bufA];
+    Node *gB = (Node *)R.grid[R.bufB];
+
+    // 1. zero this tile in the buffer the next substep will scatter into;
+    //    the flag is cleared only after every thread has read it
+    const bool zero_c = (MODE == kModeFull) && R.dirty[R.bufC][t];
+    if (zero_c) {
+        Node *gC = (Node *)R.grid[R.bufC];
+        for (int k = tid; k < TX * TY; k += nthr) {
+            int gx = x0 + k % TX, gy = y0 + k / TX;
+            if (gx < GX && gy < GY) node_zero(gC, (size_t)gy * GX + gx);
+        }
+        __syncthreads();
+        if (tid == 0) R.dirty[R.bufC][t] = 0;
+    }
+    const bool has_mass = (MODE != kModeP2GOnly) && R.dirty[R.bufA][t];
+    const int np = p1 - p0;
+    if (np == 0 && !has_mass) return;
+
+    // can any node of the region touch the indenter?
+    bool contact_possible = false;
+    if (MODE != kModeP2GOnly) {
+        double h = P.cellsize, r = sqrt(P.IndRSq);
+        double lox = rx0 * h, hix = (rx0 + RX - 1) * h, loy = ry0 * h, hiy = (ry0 + RY - 1) * h;
+        double cx = fmin(fmax(R.ind_x, lox), hix), cy = fmin(fmax(R.ind_y, loy), hiy);
+        double dx = cx - R.ind_x, dy = cy - R.ind_y;
+        contact_possible = dx * dx + dy * dy <= r * r;
+        if (contact_possible) {
+            for (int k = tid; k < 2 * P.n_indenter_subdivisions; k += nthr) s_bins[k] = 0.0;
+            if (tid == 0) { s_tot[0] = 0.0; s_tot[1] = 0.0; s_contact = 0; }
+            __syncthreads();
+        }
+    }
+    if (tid < 9) s_mark[tid] = 0;
+
+    // 2. grid update of the region (velocities into shared memory)
+    if (MODE != kModeP2GOnly) {
+        const int nloop = (np > 0) ? RN : TX * TY;
+        for (int k = tid; k < nloop; k += nthr) {
+            int gx, gy;
+            if (np > 0) { gx = rx0 + k % RX; gy = ry0 + k / RX; }
+            else { gx = x0 + k % TX; gy = y0 + k / TX; }
+            real v0 = 0, v1 = 0;
+            if (gx >= 0 && gy >= 0 && gx < GX && gy < GY) {
+                Node n = gA[(size_t)gy * GX + gx];
+                double f0 = 0, f1 = 0;
+                int bin;
+                Pol::node_velocity(P, K, n, gx, gy, R.ind_x, R.ind_y, v0, v1, f0, f1, bin);
+                bool own = gx >= x0 && gx < x0 + TX && gy >= y0 && gy < y0 + TY;
+                if (bin >= 0 && own) {
+                    atomicAdd(&s_bins[2 * bin], f0);
+                    atomicAdd(&s_bins[2 * bin + 1], f1);
+                    atomicAdd(&s_tot[0], f0);
+                    atomicAdd(&s_tot[1], f1);
+                    s_contact = 1;
+                }
+            }
+            if (np > 0) { s_v0[k] = v0; s_v1[k] = v1; }
+        }
+    }
+    if (MODE != kModeFinal)
+        for (int k = tid; k < RN; k += nthr) { s_am[k] = 0; s_ax[k] = 0; s_ay[k] = 0; }
+    __syncthreads();
+    if (MODE != kModeP2GOnly && contact_possible && s_contact) {
+        for (int k = tid; k < 2 * P.n_indenter_subdivisions; k += nthr)
+            if (s_bins[k] != 0.0) atomicAdd(&R.bins[k], s_bins[k]);
+        if (tid == 0 && R.force_slot) {
+            atomicAdd(&R.force_slot[0], s_tot[0]);
+            atomicAdd(&R.force_slot[1], s_tot[1]);
+        }
+    }
+    if (np == 0) return;
+
+    // 3.-4. particles
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+    const real h = Pol::h(P, K), m = Pol::mass(P, K), fhi = Pol::four_h_inv(P, K);
+    int bad = 0;
+    unsigned redo_count = 0;
+    for (int pb = p0 + warp * 32; pb < p1; pb += nwarps * 32) {
+        const int p = pb + lane;
+        const bool act = p < p1;
+        typename Pol::St s;
+        real v0 = 0, v1 = 0, B[4] = {0, 0, 0, 0};
+        if (act) {
+            s = Pol::load(A, p);
+            typename Pol::St old = s;
+            if (MODE == kModeP2GOnly) {
+                auto vv = A.vel[p];
+                auto bb = A.Bp[p];
+                v0 = vv.x; v1 = vv.y;
+                B[0] = bb.x; B[1] = bb.y; B[2] = bb.z; B[3] = bb.w;
+            } else {
+                typename Pol::Sten st = Pol::stencil(P, K, s);
+                int lx = st.bx - rx0, ly = st.by - ry0;
+                bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 && st.by >= 0 &&
+                              st.bx + 2 < GX && st.by + 2 < GY;
+#pragma unroll
+                for (int i = 0; i < 3; i++)
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        real n0, n1;
+                        if (inside) {
+                            int q = (ly + j) * RX + lx + i;
+                            n0 = s_v0[q]; n1 = s_v1[q];
+                        } else {
+                            int gx = st.bx + i, gy = st.by + j;
+                            n0 = 0; n1 = 0;
+                            if (gx >= 0 && gy >= 0 && gx < GX && gy < GY) {
+                                Node n = gA[(size_t)gy * GX + gx];
+                                double f0, f1;
+                                int bin;
+                                Pol::node_velocity(P, K, n, gx, gy, R.ind_x, R.ind_y, n0, n1, f0, f1, bin);
+                            }
+                        }
+                        real W = st.wx[i] * st.wy[j];
+                        real d0 = (real)i - st.fx, d1 = (real)j - st.fy;
+                        v0 += W * n0;
+                        v1 += W * n1;
+                        real c = fhi * W;
+                        B[0] += c * (n0 * d0);
+                        B[1] += c * (n0 * d1);
+                        B[2] += c * (n1 * d0);
+                        B[3] += c * (n1 * d1);
+                    }
+                real p_tr, q_tr;
+                int redo;
+                Pol::advance(P, K, s, v0, v1, B, p_tr, q_tr, redo);
+                redo_count += redo;
+                Pol::store(A, p, s, old);
+                if (R.record_pq) A.pq[p] = {p_tr, q_tr};
+                if (MODE == kModeFinal) {
+                    A.vel[p] = {v0, v1};
+                    A.Bp[p] = {B[0], B[1], B[2], B[3]};
+                }
+            }
+        }
+        if (MODE == kModeFinal) continue;
+
+        // P2G of the (updated) particle
+        real cm[9], cx[9], cy[9];
+        int key = -1 - lane;
+        bool fallback = false;
+        typename Pol::Sten st;
+        if (act) {
+            real S[4];
+            Pol::p2g_matrix(P, K, s, B, S);
+            st = Pol::stencil(P, K, s);
+            real mv0 = v0 * m, mv1 = v1 * m;
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    real W = st.wx[i] * st.wy[j];
+                    real d0 = ((real)i - st.fx) * h, d1 = ((real)j - st.fy) * h;
+                    cm[i * 3 + j] = W * m;
+                    cx[i * 3 + j] = W * (mv0 + (S[0] * d0 + S[1] * d1));
+                    cy[i * 3 + j] = W * (mv1 + (S[2] * d0 + S[3] * d1));
+                }
+            int lx = st.bx - rx0, ly = st.by - ry0;
+            if (lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 && st.by >= 0 && st.bx + 2 < GX &&
+                st.by + 2 < GY)
+                key = ly * RX + lx;
+            else
+                fallback = true;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 9; k++) { cm[k] = 0; cx[k] = 0; cy[k] = 0; }
+        }
+        bool head = true;
+        if (REDUCE) head = warp_segment_sum<9>(key, cm, cx, cy);
+        if (key >= 0 && head) {
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    int q = key + j * RX + i;
+                    atomicAdd(&s_am[q], cm[i * 3 + j]);
+                    atomicAdd(&s_ax[q], cx[i * 3 + j]);
+                    atomicAdd(&s_ay[q], cy[i * 3 + j]);
+                }
+        }
+        if (fallback) {
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    int gx = st.bx + i, gy = st.by + j;
+                    if (gx < 0 || gy < 0 || gx >= GX || gy >= GY) { bad = 1; continue; }
+                    node_add_global(gB, (size_t)gy * GX + gx, cm[i * 3 + j], cx[i * 3 + j], cy[i * 3 + j]);
+                    R.dirty[R.bufB][(gy / TY) * R.ntx + gx / TX] = 1;
+                }
+        }
+    }
+    if (bad) *R.err = 1;
+    if (redo_count && R.fp64_redo) atomicAdd(R.fp64_redo, (unsigned long long)redo_count);
+    if (MODE == kModeFinal) return;
+    __syncthreads();
+
+    // 5. add the shared region to the scatter buffer
+    for (int k = tid; k < RN; k += nthr) {
+        real mm = s_am[k];
+        if (mm == 0) continue;
+        int gx = rx0 + k % RX, gy = ry0 + k / RX;
+        if (gx < 0 || gy < 0 || gx >= GX || gy >= GY) continue;  // unreachable: such stencils take the fallback
+        node_add_global(gB, (size_t)gy * GX + gx, mm, s_ax[k], s_ay[k]);
+        int dtx = gx / TX - tx + 1, dty = gy / TY - ty + 1;
+        s_mark[dty * 3 + dtx] = 1;
+    }
+    __syncthreads();
+    if (tid < 9 && s_mark[tid]) {
+        int ntx2 = tx + tid % 3 - 1, nty2 = ty + tid / 3 - 1;
+        if (ntx2 >= 0 && nty2 >= 0 && ntx2 < R.ntx && nty2 < R.nty) R.dirty[R.bufB][nty2 * R.ntx + ntx2] = 1;
+    }
+}
+
+// ------------------------------------------------ binning, pack and unpack
+
+struct TileGeom { int TX, TY, ntx, nty; };
+
+// base node of a reference-layout particle, clamped into the grid
+__device__ __forceinline__ int sort_key(const icy_SimParams &P, const TileGeom &g, double x, double y)
+{
+    int bx = (int)(x * P.cellsize_inv - 0.5), by = (int)(y * P.cellsize_inv - 0.5);
+    bx = min(max(bx, 0), P.GridX - 1);
+    by = min(max(by, 0), P.GridY - 1);
+    int tx = bx / g.TX, ty = by / g.TY;
+    return ((ty * g.ntx + tx) * g.TY + (by - ty * g.TY)) * g.TX + (bx - tx * g.TX);
+}
+
+__global__ void k_bin_keys(const icy_SimParams P, const TileGeom g, int *key, int *count)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.nPts) return;
+    const double *pts = P.pts_array;
+    double x = pts[(size_t)ICM_IDX_POSX * P.nPtsPitch + i];
+    double y = pts[(size_t)(ICM_IDX_POSX + 1) * P.nPtsPitch + i];
+    int k = sort_key(P, g, x, y);
+    key[i] = k;
+    atomicAdd(&count[k], 1);
+}
+
+// exclusive scan, 3 phases over chunks of 4*1024 ints
+constexpr int kScanThreads = 1024, kScanItems = 4, kScanChunk = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int *tmp, int &total)
+{
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) tmp[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        int s = lane < nw ? tmp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < nw) tmp[lane] = s;
+    }
+    __syncthreads();
+    int before = (w > 0 ? tmp[w - 1] : 0) + x - v;
+    total = tmp[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_chunks(const int *in, int n, int *chunk_sums)
+{
+    __shared__ int tmp[32];
+    int base = blockIdx.x * kScanChunk + threadIdx.x * kScanItems;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+        if (base + k < n) s += in[base + k];
+    int total;
+    block_exclusive_scan(s, tmp, total);
+    if (threadIdx.x == 0) chunk_sums[blockIdx.x] = total;
+}
+
+// single block: exclusive scan of up to kScanChunk chunk sums in place
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int *sums, int n)
+{
+    __shared__ int tmp[32];
+    int base = threadIdx.x * kScanItems;
+    int v[kScanItems], s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = (base + k < n) ? sums[base + k] : 0;
+        s += v[k];
+    }
+    int total;
+    int before = block_exclusive_scan(s, tmp, total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < n) sums[base + k] = before;
+        before += v[k];
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int *in, int n, const int *chunk_off, int *out)
+{
+    __shared__ int tmp[32];
+    int base = blockIdx.x * kScanChunk + threadIdx.x * kScanItems;
+    int v[kScanItems], s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        s += v[k];
+    }
+    int total;
+    int before = block_exclusive_scan(s, tmp, total) + chunk_off[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < n) out[base + k] = before;
+        before += v[k];
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) out[n] = before;
+}
+
+__global__ void k_bin_scatter(int n, const int *key, int *cursor, int *perm)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int pos = atomicAdd(&cursor[key[i]], 1);
+    perm[pos] = i;
+}
+
+// Restores particle order inside every cell (atomic scatter order is not
+// deterministic): insertion sort of the few indices of each cell.
+__global__ void k_bin_order(int ncells, const int *start, int *perm)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int a = start[c], b = start[c + 1];
+    for (int i = a + 1; i < b; i++) {
+        int v = perm[i], j = i - 1;
+        while (j >= a && perm[j] > v) { perm[j + 1] = perm[j]; j--; }
+        perm[j + 1] = v;
+    }
+}
+
+__global__ void k_tile_starts(int ntiles, int cells_per_tile, const int *cell_start, int *tile_start)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t <= ntiles) tile_start[t] = cell_start[t * cells_per_tile];
+}
+
+__device__ __forceinline__ uint32_t read_meta(const icy_SimParams &P, int i)
+{
+    const uint8_t *cr = (const uint8_t *)P.pts_array;
+    const uint16_t *gr = (const uint16_t *)((const char *)P.pts_array + P.nPtsPitch);
+    return (uint32_t)gr[i] | ((uint32_t)cr[i] << 16);
+}
+
+__global__ void k_pack64(const icy_SimParams P, const int *perm, int *pid, Parts64 A)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.nPts) return;
+    int i = perm[k];
+    const double *pts = P.pts_array;
+    const size_t pp = P.nPtsPitch;
+    auto row = [&](int r) { return pts[(size_t)r * pp + i]; };
+    pid[k] = i;
+    A.pos[k] = make_double2(row(ICM_IDX_POSX), row(ICM_IDX_POSX + 1));
+    A.vel[k] = make_double2(row(ICM_IDX_VELX), row(ICM_IDX_VELX + 1));
+    A.F[k] = make_double4(row(ICM_IDX_FE00), row(ICM_IDX_FE00 + 1), row(ICM_IDX_FE00 + 2), row(ICM_IDX_FE00 + 3));
+    A.Bp[k] = make_double4(row(ICM_IDX_BP00), row(ICM_IDX_BP00 + 1), row(ICM_IDX_BP00 + 2), row(ICM_IDX_BP00 + 3));
+    A.Jp[k] = row(ICM_IDX_JP_INV);
+    A.meta[k] = read_meta(P, i);
+}
+
+__global__ void k_unpack64(const icy_SimParams P, const int *pid, const Parts64 A, int write_pq)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.nPts) return;
+    int i = pid[k];
+    double *pts = P.pts_array;
+    const size_t pp = P.nPtsPitch;
+    auto row = [&](int r) -> double & { return pts[(size_t)r * pp + i]; };
+    double2 x = A.pos[k], v = A.vel[k];
+    double4 F = A.F[k], B = A.Bp[k];
+    row(ICM_IDX_POSX) = x.x; row(ICM_IDX_POSX + 1) = x.y;
+    row(ICM_IDX_VELX) = v.x; row(ICM_IDX_VELX + 1) = v.y;
+    row(ICM_IDX_FE00) = F.x; row(ICM_IDX_FE00 + 1) = F.y; row(ICM_IDX_FE00 + 2) = F.z; row(ICM_IDX_FE00 + 3) = F.w;
+    row(ICM_IDX_BP00) = B.x; row(ICM_IDX_BP00 + 1) = B.y; row(ICM_IDX_BP00 + 2) = B.z; row(ICM_IDX_BP00 + 3) = B.w;
+    row(ICM_IDX_JP_INV) = A.Jp[k];
+    ((uint8_t *)pts)[i] = (uint8_t)(A.meta[k] >> 16);
+    if (write_pq) {
+        double2 q = A.pq[k];
+        row(ICM_IDX_P) = q.x;
+        row(ICM_IDX_Q) = q.y;
+    }
+}
+
+__global__ void k_pack32(const icy_SimParams P, const int *perm, int *pid, Parts32 A)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.nPts) return;
+    int i = perm[k];
+    const double *pts = P.pts_array;
+    const size_t pp = P.nPtsPitch;
+    auto row = [&](int r) { return pts[(size_t)r * pp + i]; };
+    pid[k] = i;
+    double X = row(ICM_IDX_POSX) * P.cellsize_inv, Y = row(ICM_IDX_POSX + 1) * P.cellsize_inv;
+    double fx = floor(X), fy = floor(Y);
+    float rx = (float)(X - fx), ry = (float)(Y - fy);
+    int ix = (int)fx, iy = (int)fy;
+    if (rx >= 1.0f) { rx = 0.0f; ix += 1; }
+    if (ry >= 1.0f) { ry = 0.0f; iy += 1; }
+    A.cell[k] = pack_cell(ix, iy);
+    A.frac[k] = make_float2(rx, ry);
+    A.vel[k] = make_float2((float)row(ICM_IDX_VELX), (float)row(ICM_IDX_VELX + 1));
+    A.H[k] = make_float4((float)(row(ICM_IDX_FE00) - 1.0), (float)row(ICM_IDX_FE00 + 1), (float)row(ICM_IDX_FE00 + 2),
+                         (float)(row(ICM_IDX_FE00 + 3) - 1.0));
+    A.Bp[k] = make_float4((float)row(ICM_IDX_BP00), (float)row(ICM_IDX_BP00 + 1), (float)row(ICM_IDX_BP00 + 2),
+                          (float)row(ICM_IDX_BP00 + 3));
+    A.Jp[k] = (float)row(ICM_IDX_JP_INV);
+    A.meta[k] = read_meta(P, i);
+}
+
+__global__ void k_unpack32(const icy_SimParams P, const int *pid, const Parts32 A, int write_pq)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= P.nPts) return;
+    int i = pid[k];
+    double *pts = P.pts_array;
+    const size_t pp = P.nPtsPitch;
+    auto row = [&](int r) -> double & { return pts[(size_t)r * pp + i]; };
+    uint32_t c = A.cell[k];
+    float2 f = A.frac[k], v = A.vel[k];
+    float4 H = A.H[k], B = A.Bp[k];
+    row(ICM_IDX_POSX) = ((double)cell_x(c) + (double)f.x) * P.cellsize;
+    row(ICM_IDX_POSX + 1) = ((double)cell_y(c) + (double)f.y) * P.cellsize;
+    row(ICM_IDX_VELX) = v.x; row(ICM_IDX_VELX + 1) = v.y;
+    row(ICM_IDX_FE00) = 1.0 + (double)H.x; row(ICM_IDX_FE00 + 1) = H.y;
+    row(ICM_IDX_FE00 + 2) = H.z; row(ICM_IDX_FE00 + 3) = 1.0 + (double)H.w;
+    row(ICM_IDX_BP00) = B.x; row(ICM_IDX_BP00 + 1) = B.y; row(ICM_IDX_BP00 + 2) = B.z; row(ICM_IDX_BP00 + 3) = B.w;
+    row(ICM_IDX_JP_INV) = A.Jp[k];
+    ((uint8_t *)pts)[i] = (uint8_t)(A.meta[k] >> 16);
+    if (write_pq) {
+        float2 q = A.pq[k];
+        row(ICM_IDX_P) = q.x;
+        row(ICM_IDX_Q) = q.y;
+    }
+}
+
+}  // namespace icm

@@ -1,0 +1,178 @@
+/*
+ * icempm.h -- C ABI of the B200 MLS-MPM substep library (libicempm.so).
+ *
+ * This is the drop-in boundary for iceMPM's device layer, the C++ class
+ * GPU_Implementation5 (simulation/gpu_implementation5.h:40-72) and the step
+ * loop that drives it (icy::Model::Step, simulation/model.cpp:11-47). Every
+ * entry point takes plain pointers and sizes, returns ICM_OK (0) or an
+ * ICM_ERR_* code and never throws; icm_last_error() gives the message of the
+ * calling thread's last failure. The C++ shim in include/icempm.hpp turns a
+ * non-zero status back into std::runtime_error, which is what the reference
+ * members do (gpu_implementation5.cu:458-592).
+ *
+ * Buffers follow the reference:
+ *   particles  16 rows x nPtsPitch doubles (parameters_sim.h:27-35), row 0
+ *              holding the crushed byte at byte i and the grain id (int16)
+ *              at byte offset nPtsPitch + 2*i (point.cpp:19-23);
+ *   grid       3 rows x nGridPitch doubles: mass, momentum|velocity x, y;
+ *   force bins 2*n_indenter_subdivisions doubles, accumulated over a frame.
+ * Pitches are in elements and are written into SimParams by
+ * icm_allocate_arrays, as cudaMallocPitch results are in the reference.
+ */
+#ifndef ICEMPM_H
+#define ICEMPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "icempm_params.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    ICM_OK = 0,
+    ICM_ERR_CUDA = 1,      /* a CUDA runtime call failed */
+    ICM_ERR_ARG = 2,       /* bad argument (null pointer, size out of range) */
+    ICM_ERR_STATE = 3,     /* call out of order (e.g. no arrays allocated) */
+    ICM_ERR_NOMEM = 4,     /* device or host allocation failed */
+    ICM_ERR_IO = 5,        /* file missing or unreadable */
+    ICM_ERR_PARSE = 6,     /* configuration not valid JSON / missing key */
+    ICM_ERR_NODEVICE = 7   /* no CUDA device */
+};
+
+/* Precision / execution forms of icm_run_substeps. */
+enum {
+    ICM_FORM_FP64_STEPWISE = 0, /* reference structure: reset, P2G, update, G2P launches per substep, FP64 */
+    ICM_FORM_FP64 = 1,          /* fused tile substep, FP64 reference form */
+    ICM_FORM_FP32 = 2           /* fused tile substep, FP32 strain form */
+};
+
+typedef struct icm_ctx icm_ctx;
+typedef void (*icm_host_fn)(void *user);
+
+const char *icm_last_error(void);
+const char *icm_version(void);
+
+/* ---------------------------------------------------------- SimParams
+ * parameters_sim.cpp: Reset :5-56, ParseFile :59-119, ComputeLame :121-126,
+ * ComputeHelperVariables :128-136, ComputeCamClayParams2 :138-147,
+ * ComputeIntegerBlockCoords :149-155. */
+void icm_params_reset(icy_SimParams *p);
+/* Parses a flat JSON object (the keys of parameters_sim.cpp:73-99) and
+ * recomputes the derived values. Copies "InputRawPoints" into raw_points
+ * (may be NULL); returns ICM_ERR_PARSE if that key is missing, as ParseFile
+ * throws "config parameter missing" (parameters_sim.cpp:110-114). */
+int icm_params_parse_file(icy_SimParams *p, const char *path, char *raw_points, size_t cap);
+int icm_params_parse_string(icy_SimParams *p, const char *json, char *raw_points, size_t cap);
+void icm_params_compute_lame(icy_SimParams *p);
+void icm_params_compute_camclay(icy_SimParams *p);
+void icm_params_compute_helpers(icy_SimParams *p);
+void icm_params_compute_block_coords(icy_SimParams *p);
+/* Pitch (elements) used for an array of n doubles: n rounded up to 64. */
+size_t icm_pitch_elems(size_t n);
+
+/* ------------------------------------------------ synthetic ice block
+ * Stands in for SnapshotManager::LoadRawPoints (snapshotmanager.cpp:186-286)
+ * when no HDF5 point cloud is given: a block of cells_x x cells_y cells at
+ * 2x2 jittered sites per cell (jitter +-0.25 sub-cell), seeded Voronoi grains
+ * (about one per grain_size metres), sorted by grid cell as SortPoints does
+ * (snapshotmanager.cpp:288-304). Sets nPts, Volume, bounding box,
+ * ParticleVolume, ParticleMass and the indenter start: x = block_left - r,
+ * y = block_bottom + ind_y_above_floor. Fills host_soa (16 x pitch doubles,
+ * pitch = icm_pitch_elems(n)) when it is not NULL; returns the particle
+ * count through n_out. */
+typedef struct icm_block_desc {
+    int cells_x, cells_y;       /* block size in grid cells */
+    double ind_y_above_floor;   /* indenter centre above the block bottom, metres */
+    double grain_size;          /* metres per Voronoi grain */
+    uint64_t seed;
+} icm_block_desc;
+int icm_scene_block(icy_SimParams *p, const icm_block_desc *d, double *host_soa, int *n_out);
+
+/* -------------------------------------------------------- device layer */
+
+/* GPU_Implementation5::initialize (gpu_implementation5.cu:452-469). */
+int icm_create(icm_ctx **out, int device);
+/* Frees device and host buffers the context owns (the reference has no
+ * destructor). */
+int icm_destroy(icm_ctx *ctx);
+/* Selects the form used by icm_run_substeps (an extension of SimParams'
+ * role; the reference has only the FP64 stepwise form). */
+int icm_set_form(icm_ctx *ctx, int form);
+int icm_get_form(icm_ctx *ctx);
+/* Tile shape of the fused forms: index into the built variants
+ * (0: 16x8, 1: 16x16, 2: 32x8, 3: 32x16 nodes) and block size. */
+int icm_set_tile(icm_ctx *ctx, int tile_variant, int threads);
+int icm_get_tile(icm_ctx *ctx, int *tile_variant, int *threads);
+/* GPU_Implementation5::cuda_allocate_arrays (gpu_implementation5.cu:481-513):
+ * device particle SoA, grid and force bins. Writes the device pointers and
+ * pitches into *p and resets the error code. */
+int icm_allocate_arrays(icm_ctx *ctx, icy_SimParams *p, size_t n_grid_nodes, size_t n_points);
+/* GPU_Implementation5::cuda_update_constants (gpu_implementation5.cu:471-479):
+ * takes a copy of *p for the kernels and writes error_code to the device
+ * error word. */
+int icm_update_constants(icm_ctx *ctx, const icy_SimParams *p, int error_code);
+/* GPU_Implementation5::transfer_ponts_to_device (gpu_implementation5.cu:515-526). */
+int icm_transfer_points_to_device(icm_ctx *ctx, const double *host_soa);
+/* GPU_Implementation5::cuda_reset_grid (gpu_implementation5.cu:554-559). */
+int icm_reset_grid(icm_ctx *ctx);
+/* GPU_Implementation5::cuda_reset_indenter_force_accumulator (:561-565). */
+int icm_reset_indenter_force_accumulator(icm_ctx *ctx);
+/* GPU_Implementation5::cuda_p2g (gpu_implementation5.cu:568-575). */
+int icm_p2g(icm_ctx *ctx);
+/* GPU_Implementation5::cuda_update_nodes (gpu_implementation5.cu:577-584). */
+int icm_update_nodes(icm_ctx *ctx, double indenter_x, double indenter_y);
+/* GPU_Implementation5::cuda_g2p (gpu_implementation5.cu:586-593). */
+int icm_g2p(icm_ctx *ctx, int record_pq);
+/* GPU_Implementation5::cuda_transfer_from_device (gpu_implementation5.cu:528-544):
+ * enqueues the copies of the particle SoA (host_soa may be NULL), the force
+ * bins (host_bins may be NULL) and the error word, then the host function
+ * cb(user) (the stream callback of :542-552; it must not call CUDA). The
+ * copies complete asynchronously: call icm_synchronize or wait for cb. */
+int icm_transfer_from_device(icm_ctx *ctx, double *host_soa, double *host_bins, int *error_code,
+                             icm_host_fn cb, void *user);
+/* Copies of the reference-layout grid (3 rows x nGridPitch doubles). The
+ * reference keeps the grid private to its kernels; these serve callers and
+ * tests that drive the member-style kernels one by one. Synchronous. */
+int icm_transfer_grid_to_device(icm_ctx *ctx, const double *host_grid);
+int icm_transfer_grid_from_device(icm_ctx *ctx, double *host_grid);
+/* GPU_Implementation5::synchronize (gpu_implementation5.cu:442-446). */
+int icm_synchronize(icm_ctx *ctx);
+/* The substep loop of icy::Model::Step (model.cpp:20-29): n substeps of
+ * t += dt; indenter_x = indenter_x_initial + t*IndVelocity; reset; P2G;
+ * update; G2P, with P and Q recorded on every substep that ends a frame
+ * ((SimulationStep + k) % UpdateEveryNthStep == 0). Runs in the form set by
+ * icm_set_form, advances p->SimulationStep, SimulationTime and indenter_x,
+ * and keeps each substep's summed indenter reaction (see
+ * icm_force_history). Asynchronous on the context's stream. */
+int icm_run_substeps(icm_ctx *ctx, icy_SimParams *p, int n);
+/* Copies the per-substep reaction totals (2 doubles each) of the last
+ * icm_run_substeps into host_out (synchronous). */
+int icm_force_history(icm_ctx *ctx, double *host_out, int n);
+/* Number of particles the FP32 form handed to the FP64 fallback since the
+ * context was created (synchronous). */
+int icm_fp64_redo_count(icm_ctx *ctx, unsigned long long *out);
+/* CUDA events around work on the context's stream (eventCycleStart/Stop of
+ * gpu_implementation5.h:61). */
+int icm_record_start(icm_ctx *ctx);
+int icm_record_stop(icm_ctx *ctx);
+int icm_elapsed_ms(icm_ctx *ctx, float *ms);
+/* Per-launch timing of the fused substep kernel: when enabled, every
+ * steady-state launch of icm_run_substeps is bracketed by a CUDA event pair
+ * on the context's stream; icm_kernel_time returns the summed durations and
+ * the launch count since enabling (synchronises). */
+int icm_kernel_timing(icm_ctx *ctx, int enable);
+int icm_kernel_time(icm_ctx *ctx, double *total_ms, long long *launches);
+/* The context's CUDA stream (cudaStream_t) for callers that interleave
+ * their own work. */
+void *icm_stream(icm_ctx *ctx);
+/* Pinned host memory for transfer buffers (cudaMallocHost/cudaFreeHost). */
+int icm_host_alloc(void **ptr, size_t bytes);
+int icm_host_free(void *ptr);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* ICEMPM_H */

@@ -1,0 +1,122 @@
+"""ctypes loader of the CPU FP64 oracle (oracle/mpm_oracle.c).
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference legs, as the checker. The product path
+never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmpm_oracle.so")
+REF_SVD_PATH = os.path.join(HERE, "_ref", "libref_svd.so")
+
+_L = None
+
+
+def lib():
+    global _L
+    if _L is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: run `make -C oracle`")
+        from icempm_b200 import SimParams
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER(SimParams)
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        sigs = {
+            "oracle_svd2x2": (None, [vp, vp, vp, vp]),
+            "oracle_kirchhoff": (None, [P, vp, vp]),
+            "oracle_constitutive": (None, [P, vp, vp, vp, C.c_short, vp, vp]),
+            "oracle_reset_grid": (None, [P, vp]),
+            "oracle_p2g": (i, [P, vp, vp, i]),
+            "oracle_update_nodes": (None, [P, vp, vp, d, d, vp, i]),
+            "oracle_g2p": (None, [P, vp, vp, i, i]),
+            "oracle_run_substeps": (i, [P, vp, vp, vp, vp, i, i]),
+            "oracle_max_threads": (i, []),
+        }
+        for n, (r, a) in sigs.items():
+            f = getattr(L, n)
+            f.restype = r
+            f.argtypes = a
+        _L = L
+    return _L
+
+
+def ref_svd_lib():
+    """The reference's own SVD compiled for the host, or None if not built."""
+    if not os.path.exists(REF_SVD_PATH):
+        return None
+    L = C.CDLL(REF_SVD_PATH)
+    L.ref_svd.restype = None
+    L.ref_svd.argtypes = [C.c_void_p] * 4
+    return L
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data
+
+
+def svd2x2(A):
+    """Row-major 2x2 -> (U row-major, sigma, V row-major) as the reference's
+    svd2x2_modified returns them."""
+    A = np.ascontiguousarray(A, dtype=np.float64).reshape(4)
+    U, S, V = np.zeros(4), np.zeros(2), np.zeros(4)
+    lib().oracle_svd2x2(_p(A), _p(U), _p(S), _p(V))
+    return U, S, V
+
+
+def constitutive(prms, Fe, Jp_inv, crushed, grain):
+    Fe = np.ascontiguousarray(Fe, dtype=np.float64).reshape(4).copy()
+    jp = np.array([Jp_inv], dtype=np.float64)
+    cr = np.array([crushed], dtype=np.uint8)
+    p = np.zeros(1)
+    q = np.zeros(1)
+    lib().oracle_constitutive(C.byref(prms), _p(Fe), _p(jp), cr.ctypes.data, int(grain), _p(p), _p(q))
+    return Fe, float(jp[0]), int(cr[0]), float(p[0]), float(q[0])
+
+
+def kirchhoff(prms, F):
+    F = np.ascontiguousarray(F, dtype=np.float64).reshape(4)
+    tau = np.zeros(4)
+    lib().oracle_kirchhoff(C.byref(prms), _p(F), _p(tau))
+    return tau
+
+
+def new_grid(prms) -> np.ndarray:
+    return np.zeros(int(prms.nGridPitch) * 3, dtype=np.float64)
+
+
+def reset_grid(prms, grid):
+    lib().oracle_reset_grid(C.byref(prms), _p(grid))
+
+
+def p2g(prms, pts, grid, threads=1) -> int:
+    return int(lib().oracle_p2g(C.byref(prms), _p(pts), _p(grid), threads))
+
+
+def update_nodes(prms, grid, bins, ix, iy, threads=1):
+    tot = np.zeros(2)
+    lib().oracle_update_nodes(C.byref(prms), _p(grid), _p(bins), ix, iy, _p(tot), threads)
+    return tot
+
+
+def g2p(prms, pts, grid, record_pq, threads=1):
+    lib().oracle_g2p(C.byref(prms), _p(pts), _p(grid), 1 if record_pq else 0, threads)
+
+
+def run_substeps(prms, pts, grid, bins, n, threads=1, history=True):
+    """Model::Step's substep loop on the CPU; returns (error, force history
+    [n, 2] or None). Advances prms.SimulationStep / SimulationTime."""
+    hist = np.zeros(2 * n) if history else None
+    err = lib().oracle_run_substeps(C.byref(prms), _p(pts), _p(grid), _p(bins),
+                                    _p(hist) if history else None, n, threads)
+    return int(err), (hist.reshape(n, 2) if history else None)
+
+
+def max_threads() -> int:
+    return int(lib().oracle_max_threads())
