@@ -43,7 +43,7 @@ def parse():
     a.add_argument("--config", default="c3_1m")
     a.add_argument("--substeps", type=int, default=100)
     a.add_argument("--tile", type=int, default=-1, help="tile variant (-1: autotuned)")
-    a.add_argument("--threads", type=int, default=256)
+    a.add_argument("--threads", type=int, default=128)
     a.add_argument("--no-e2e", action="store_true")
     a.add_argument("--no-accuracy", action="store_true")
     a.add_argument("--no-cpu", action="store_true")

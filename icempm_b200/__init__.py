@@ -177,6 +177,7 @@ def _lib():
                 "icm_run_substeps": (i, [vp, P, i]),
                 "icm_force_history": (i, [vp, vp, i]),
                 "icm_fp64_redo_count": (i, [vp, C.POINTER(C.c_ulonglong)]),
+                "icm_stray_count": (i, [vp, C.POINTER(C.c_ulonglong)]),
                 "icm_record_start": (i, [vp]), "icm_record_stop": (i, [vp]),
                 "icm_elapsed_ms": (i, [vp, C.POINTER(C.c_float)]),
                 "icm_stream": (vp, [vp]),
@@ -279,7 +280,7 @@ class GPU_Implementation5:
     def get_form(self) -> int:
         return int(_lib().icm_get_form(self._ctx))
 
-    def set_tile(self, variant: int, threads: int = 256) -> None:
+    def set_tile(self, variant: int, threads: int = 128) -> None:
         self.initialize()
         _check(_lib().icm_set_tile(self._ctx, variant, threads))
 
@@ -370,6 +371,11 @@ class GPU_Implementation5:
     def fp64_redo_count(self) -> int:
         v = C.c_ulonglong(0)
         _check(_lib().icm_fp64_redo_count(self._ctx, C.byref(v)))
+        return int(v.value)
+
+    def stray_count(self) -> int:
+        v = C.c_ulonglong(0)
+        _check(_lib().icm_stray_count(self._ctx, C.byref(v)))
         return int(v.value)
 
     def record_start(self) -> None:

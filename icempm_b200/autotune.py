@@ -68,12 +68,12 @@ def choose(config_name: str, form: int, device: int = 0, substeps: int = 30):
             except (OSError, ValueError):
                 cache = {}
         if key in cache:
-            v, t = cache[key]["tile"], cache[key]["threads"]
+            c = cache[key]
             m.gpu.close()
-            return v, t, f"autotuned (cached): {cache[key]['us']:.2f} us/substep"
+            return c["tile"], c["threads"], f"autotuned (cached): {c['us']:.2f} us/substep"
     res = sweep(m, substeps=substeps)
     m.gpu.close()
-    v, t, us = min(res, key=lambda r: r[2])
+    v, t, us = min(res, key=lambda x: x[2])
     with _LOCK:
         cache[key] = {"tile": v, "threads": t, "us": us, "sweep": res}
         try:

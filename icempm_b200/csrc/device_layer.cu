@@ -66,7 +66,8 @@ void dfree(T *&p)
 struct Binning {
     int *key = nullptr, *count = nullptr, *cell_start = nullptr, *cursor = nullptr, *perm = nullptr;
     int *chunk = nullptr, *tile_start = nullptr, *pid = nullptr;
-    size_t cap_pts = 0, cap_cells = 0, cap_tiles = 0;
+    int *group_slots = nullptr, *group_base = nullptr, *gchunk = nullptr;
+    size_t cap_pts = 0, cap_cells = 0, cap_tiles = 0, cap_slots = 0;
 };
 
 struct Fused {
@@ -85,7 +86,7 @@ struct icm_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     int form = ICM_FORM_FP64_STEPWISE;
-    int tile_variant = 1, threads = 256;
+    int tile_variant = 1, threads = 128;
 
     icy_SimParams prms{};
     size_t cap_pts = 0, cap_nodes = 0, pts_pitch = 0, grid_pitch = 0;
@@ -95,6 +96,7 @@ struct icm_ctx {
     size_t hist_cap = 0;
     int hist_n = 0;
     unsigned long long *d_redo = nullptr;
+    unsigned long long *d_strays = nullptr;
 
     // optional per-launch timing of the fused substep kernel (kModeFull)
     bool ktime = false;
@@ -105,6 +107,7 @@ struct icm_ctx {
 
     bool ref_valid = true, internal_valid = false, internal_pq = false;
     int internal_variant = -1;
+    int nslots = 0;
     Binning bin;
     Fused fz;
 };
@@ -152,7 +155,6 @@ static Consts32 make_consts32(const icy_SimParams &P)
     k.stress_c = (float)((P.InitialTimeStep * P.ParticleVolume) * P.Dp_inv);
     k.mu = (float)P.mu;
     k.kappa = (float)P.kappa;
-    k.half_kappa = (float)(P.kappa / 2.);
     k.tan_phi = (float)P.DP_tan_phi;
     k.p_thr = (float)P.DP_threshold_p;
     k.pmax_dp = (float)P.IceCompressiveStrength;
@@ -163,10 +165,13 @@ static Consts32 make_consts32(const icy_SimParams &P)
     double jm1 = a / (std::sqrt(1.0 + a) + 1.0);
     k.tension_delta = (float)(jm1 / (std::sqrt(Je_new) + 1.0));
     k.gv = (float)P.GrainVariability;
-    k.ics = (float)P.IceCompressiveStrength;
-    k.its = (float)P.IceTensileStrength;
-    k.iss = (float)P.IceShearStrength;
+    k.ics = (float)(P.IceCompressiveStrength * 1e-6);
+    k.its = (float)(P.IceTensileStrength * 1e-6);
+    k.iss = (float)(P.IceShearStrength * 1e-6);
     k.four_h_inv = (float)(4.0 * P.cellsize_inv);
+    k.dt_g = (float)(P.InitialTimeStep * P.Gravity);
+    k.vmax = (float)(0.5 * P.cellsize / P.InitialTimeStep);
+    k.half_inv_mu = (float)(1.0 / (2.0 * P.mu));
     return k;
 }
 
@@ -185,6 +190,7 @@ static void free_binning(icm_ctx *c)
 {
     dfree(c->bin.key); dfree(c->bin.count); dfree(c->bin.cell_start); dfree(c->bin.cursor);
     dfree(c->bin.perm); dfree(c->bin.chunk); dfree(c->bin.tile_start); dfree(c->bin.pid);
+    dfree(c->bin.group_slots); dfree(c->bin.group_base); dfree(c->bin.gchunk);
     c->bin = Binning{};
 }
 
@@ -197,33 +203,21 @@ static void geometry(const icy_SimParams &P, int variant, TileGeom &g, int &ntil
     ntiles = g.ntx * g.nty;
 }
 
-static int ensure_fused(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t ntiles, size_t ncells)
+// Grid buffers, dirty flags and binning scratch of the fused forms.
+static int ensure_grids(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t ntiles, size_t ncells)
 {
-    if (c->fz.form != form || c->fz.cap_pts < npts || c->fz.cap_nodes < nnodes || c->fz.cap_tiles < ntiles) {
-        free_fused(c);
-        c->fz.form = form;
-        c->fz.cap_pts = npts;
+    if (c->fz.form != form || c->fz.cap_nodes < nnodes || c->fz.cap_tiles < ntiles) {
+        for (int b = 0; b < 3; b++) { if (c->fz.grid[b]) cudaFree(c->fz.grid[b]); c->fz.grid[b] = nullptr; }
+        dfree(c->fz.dirty);
         c->fz.cap_nodes = nnodes;
         c->fz.cap_tiles = ntiles;
         int rc = ICM_OK;
-        if (form == ICM_FORM_FP64) {
-            Parts64 &A = c->fz.p64;
-            if ((rc = dalloc(&A.pos, npts)) || (rc = dalloc(&A.F, npts)) || (rc = dalloc(&A.Jp, npts)) ||
-                (rc = dalloc(&A.meta, npts)) || (rc = dalloc(&A.vel, npts)) || (rc = dalloc(&A.Bp, npts)) ||
-                (rc = dalloc(&A.pq, npts)))
-                return rc;
-            for (int b = 0; b < 3; b++) {
+        for (int b = 0; b < 3; b++) {
+            if (form == ICM_FORM_FP64) {
                 Node64 *g;
                 if ((rc = dalloc(&g, nnodes))) return rc;
                 c->fz.grid[b] = g;
-            }
-        } else {
-            Parts32 &A = c->fz.p32;
-            if ((rc = dalloc(&A.cell, npts)) || (rc = dalloc(&A.frac, npts)) || (rc = dalloc(&A.H, npts)) ||
-                (rc = dalloc(&A.Jp, npts)) || (rc = dalloc(&A.meta, npts)) || (rc = dalloc(&A.vel, npts)) ||
-                (rc = dalloc(&A.Bp, npts)) || (rc = dalloc(&A.pq, npts)))
-                return rc;
-            for (int b = 0; b < 3; b++) {
+            } else {
                 float4 *g;
                 if ((rc = dalloc(&g, nnodes))) return rc;
                 c->fz.grid[b] = g;
@@ -232,18 +226,74 @@ static int ensure_fused(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t
         if ((rc = dalloc(&c->fz.dirty, 3 * ntiles))) return rc;
     }
     if (c->bin.cap_pts < npts || c->bin.cap_cells < ncells || c->bin.cap_tiles < ntiles) {
+        int *pid = c->bin.pid;  // slot-sized, managed by ensure_slots
+        size_t cap_slots = c->bin.cap_slots;
+        c->bin.pid = nullptr;
         free_binning(c);
+        c->bin.pid = pid;
+        c->bin.cap_slots = cap_slots;
         int rc;
         size_t nchunks = (ncells + kScanChunk - 1) / kScanChunk;
-        if ((rc = dalloc(&c->bin.key, npts)) || (rc = dalloc(&c->bin.perm, npts)) || (rc = dalloc(&c->bin.pid, npts)) ||
+        size_t ngroups = ncells / 32;
+        size_t ngchunks = (ngroups + kScanChunk - 1) / kScanChunk;
+        if ((rc = dalloc(&c->bin.key, npts)) || (rc = dalloc(&c->bin.perm, npts)) ||
             (rc = dalloc(&c->bin.count, ncells + 1)) || (rc = dalloc(&c->bin.cell_start, ncells + 1)) ||
             (rc = dalloc(&c->bin.cursor, ncells + 1)) || (rc = dalloc(&c->bin.chunk, nchunks + 1)) ||
-            (rc = dalloc(&c->bin.tile_start, ntiles + 1)))
+            (rc = dalloc(&c->bin.tile_start, ntiles + 1)) || (rc = dalloc(&c->bin.group_slots, ngroups + 1)) ||
+            (rc = dalloc(&c->bin.group_base, ngroups + 1)) || (rc = dalloc(&c->bin.gchunk, ngchunks + 1)))
             return rc;
         c->bin.cap_pts = npts;
         c->bin.cap_cells = ncells;
         c->bin.cap_tiles = ntiles;
     }
+    return ICM_OK;
+}
+
+// Slot-ordered particle arrays of one form (and the slot -> particle map).
+static int ensure_slots(icm_ctx *c, int form, size_t nslots)
+{
+    if (c->fz.form == form && c->fz.cap_pts >= nslots && c->bin.cap_slots >= nslots) return ICM_OK;
+    dfree(c->fz.p64.pos); dfree(c->fz.p64.F); dfree(c->fz.p64.Jp); dfree(c->fz.p64.meta);
+    dfree(c->fz.p64.vel); dfree(c->fz.p64.Bp); dfree(c->fz.p64.pq);
+    dfree(c->fz.p32.cell); dfree(c->fz.p32.frac); dfree(c->fz.p32.H); dfree(c->fz.p32.Jp);
+    dfree(c->fz.p32.meta); dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
+    dfree(c->bin.pid);
+    c->fz.form = form;
+    c->fz.cap_pts = nslots;
+    c->bin.cap_slots = nslots;
+    int rc = ICM_OK;
+    if ((rc = dalloc(&c->bin.pid, nslots))) return rc;
+    if (form == ICM_FORM_FP64) {
+        Parts64 &A = c->fz.p64;
+        if ((rc = dalloc(&A.pos, nslots)) || (rc = dalloc(&A.F, nslots)) || (rc = dalloc(&A.Jp, nslots)) ||
+            (rc = dalloc(&A.meta, nslots)) || (rc = dalloc(&A.vel, nslots)) || (rc = dalloc(&A.Bp, nslots)) ||
+            (rc = dalloc(&A.pq, nslots)))
+            return rc;
+    } else {
+        Parts32 &A = c->fz.p32;
+        if ((rc = dalloc(&A.cell, nslots)) || (rc = dalloc(&A.frac, nslots)) || (rc = dalloc(&A.H, nslots)) ||
+            (rc = dalloc(&A.Jp, nslots)) || (rc = dalloc(&A.meta, nslots)) || (rc = dalloc(&A.vel, nslots)) ||
+            (rc = dalloc(&A.Bp, nslots)) || (rc = dalloc(&A.pq, nslots)))
+            return rc;
+    }
+    return ICM_OK;
+}
+
+// Exclusive scan of n ints (n + 1 outputs) with the chunked scan kernels.
+static int scan_ints(icm_ctx *c, const int *in, int n, int *chunk, int *out)
+{
+    const int nchunks = (n + kScanChunk - 1) / kScanChunk;
+    if (nchunks > kScanChunk) return icm::fail(ICM_ERR_ARG, "scan too large");
+    if (n == 0) {
+        ICM_CUDA(cudaMemsetAsync(out, 0, sizeof(int), c->stream));
+        return ICM_OK;
+    }
+    k_scan_chunks<<<nchunks, kScanThreads, 0, c->stream>>>(in, n, chunk);
+    ICM_LAUNCHED("k_scan_chunks");
+    k_scan_sums<<<1, kScanThreads, 0, c->stream>>>(chunk, nchunks);
+    ICM_LAUNCHED("k_scan_sums");
+    k_scan_apply<<<nchunks, kScanThreads, 0, c->stream>>>(in, n, chunk, out);
+    ICM_LAUNCHED("k_scan_apply");
     return ICM_OK;
 }
 
@@ -256,22 +306,17 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
     geometry(P, c->tile_variant, g, ntiles);
     const size_t ncells = (size_t)ntiles * g.TX * g.TY;
     if (ncells > (size_t)kScanChunk * kScanChunk) return icm::fail(ICM_ERR_ARG, "grid too large for the binning scan");
-    int rc = ensure_fused(c, c->form, (size_t)P.nPts, (size_t)P.GridX * P.GridY, (size_t)ntiles, ncells);
+    int rc = ensure_grids(c, c->form, (size_t)P.nPts, (size_t)P.GridX * P.GridY, (size_t)ntiles, ncells);
     if (rc) return rc;
     cudaStream_t s = c->stream;
     const int n = P.nPts;
-    const int nchunks = (int)((ncells + kScanChunk - 1) / kScanChunk);
+    const int ngroups = (int)(ncells / 32);
     ICM_CUDA(cudaMemsetAsync(c->bin.count, 0, sizeof(int) * (ncells + 1), s));
     if (n > 0) {
         k_bin_keys<<<(n + 255) / 256, 256, 0, s>>>(P, g, c->bin.key, c->bin.count);
         ICM_LAUNCHED("k_bin_keys");
     }
-    k_scan_chunks<<<nchunks, kScanThreads, 0, s>>>(c->bin.count, (int)ncells, c->bin.chunk);
-    ICM_LAUNCHED("k_scan_chunks");
-    k_scan_sums<<<1, kScanThreads, 0, s>>>(c->bin.chunk, nchunks);
-    ICM_LAUNCHED("k_scan_sums");
-    k_scan_apply<<<nchunks, kScanThreads, 0, s>>>(c->bin.count, (int)ncells, c->bin.chunk, c->bin.cell_start);
-    ICM_LAUNCHED("k_scan_apply");
+    if ((rc = scan_ints(c, c->bin.count, (int)ncells, c->bin.chunk, c->bin.cell_start))) return rc;
     ICM_CUDA(cudaMemcpyAsync(c->bin.cursor, c->bin.cell_start, sizeof(int) * ncells, cudaMemcpyDeviceToDevice, s));
     if (n > 0) {
         k_bin_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, c->bin.key, c->bin.cursor, c->bin.perm);
@@ -281,13 +326,24 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
     ICM_LAUNCHED("k_bin_order");
     k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start);
     ICM_LAUNCHED("k_tile_starts");
+    k_group_slots<<<(ngroups + 255) / 256, 256, 0, s>>>(ngroups, c->bin.cell_start, c->bin.group_slots);
+    ICM_LAUNCHED("k_group_slots");
+    if ((rc = scan_ints(c, c->bin.group_slots, ngroups, c->bin.gchunk, c->bin.group_base))) return rc;
+    int nslots = 0;
+    ICM_CUDA(cudaMemcpyAsync(&nslots, c->bin.group_base + ngroups, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICM_CUDA(cudaStreamSynchronize(s));
+    if ((rc = ensure_slots(c, c->form, (size_t)std::max(nslots, 1)))) return rc;
+    ICM_CUDA(cudaMemsetAsync(c->bin.pid, 0xff, sizeof(int) * (size_t)std::max(nslots, 1), s));
     if (n > 0) {
         if (c->form == ICM_FORM_FP64)
-            k_pack64<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.pid, c->fz.p64);
+            k_pack64<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.key, c->bin.cell_start, c->bin.group_base,
+                                                     c->bin.pid, c->fz.p64);
         else
-            k_pack32<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.pid, c->fz.p32);
+            k_pack32<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.key, c->bin.cell_start, c->bin.group_base,
+                                                     c->bin.pid, c->fz.p32);
         ICM_LAUNCHED("k_pack");
     }
+    c->nslots = nslots;
     c->internal_valid = true;
     c->internal_variant = c->tile_variant;
     c->internal_pq = false;
@@ -300,12 +356,12 @@ static int ensure_ref(icm_ctx *c)
     if (c->ref_valid) return ICM_OK;
     if (!c->internal_valid) return icm::fail(ICM_ERR_STATE, "no valid particle state on the device");
     const icy_SimParams P = kernel_params(c, &c->prms);
-    const int n = P.nPts;
-    if (n > 0) {
+    const int ns = c->nslots;
+    if (ns > 0 && P.nPts > 0) {
         if (c->fz.form == ICM_FORM_FP64)
-            k_unpack64<<<(n + 255) / 256, 256, 0, c->stream>>>(P, c->bin.pid, c->fz.p64, c->internal_pq ? 1 : 0);
+            k_unpack64<<<(ns + 255) / 256, 256, 0, c->stream>>>(P, ns, c->bin.pid, c->fz.p64, c->internal_pq ? 1 : 0);
         else
-            k_unpack32<<<(n + 255) / 256, 256, 0, c->stream>>>(P, c->bin.pid, c->fz.p32, c->internal_pq ? 1 : 0);
+            k_unpack32<<<(ns + 255) / 256, 256, 0, c->stream>>>(P, ns, c->bin.pid, c->fz.p32, c->internal_pq ? 1 : 0);
         ICM_LAUNCHED("k_unpack");
     }
     c->ref_valid = true;
@@ -326,18 +382,34 @@ static int ensure_hist(icm_ctx *c, int n)
 
 // ----------------------------------------------------- fused run dispatch
 
-template <class Pol, int TX, int TY, bool REDUCE>
+// Dynamic shared memory of the per-warp accumulation regions; above 48 KB
+// the kernel has to opt in once.
+template <class Pol, int TX, int TY, int MODE>
+static int launch_one(icm_ctx *c, int ntiles, const icy_SimParams &P, const typename Pol::Consts &K,
+                      const typename Pol::Parts &A, const TileRun &R)
+{
+    constexpr int RN = (TX + 4) * (TY + 4);
+    const size_t dyn = (MODE == kModeFinal) ? 0 : sizeof(typename Pol::Acc) * RN * (size_t)(c->threads / 32);
+    static size_t opted = 0;  // static + dynamic shared memory above 48 KB needs the opt-in
+    if (MODE != kModeFinal && dyn > opted) {
+        ICM_CUDA(cudaFuncSetAttribute(k_tile_substep<Pol, TX, TY, MODE>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        opted = dyn;
+    }
+    k_tile_substep<Pol, TX, TY, MODE><<<ntiles, c->threads, dyn, c->stream>>>(P, K, A, R);
+    ICM_LAUNCHED("k_tile_substep");
+    return ICM_OK;
+}
+
+template <class Pol, int TX, int TY>
 static int launch_tile(icm_ctx *c, int mode, int ntiles, const icy_SimParams &P, const typename Pol::Consts &K,
                        const typename Pol::Parts &A, const TileRun &R)
 {
-    dim3 grid(ntiles), block(c->threads);
     switch (mode) {
-    case kModeP2GOnly: k_tile_substep<Pol, TX, TY, kModeP2GOnly, REDUCE><<<grid, block, 0, c->stream>>>(P, K, A, R); break;
-    case kModeFull: k_tile_substep<Pol, TX, TY, kModeFull, REDUCE><<<grid, block, 0, c->stream>>>(P, K, A, R); break;
-    default: k_tile_substep<Pol, TX, TY, kModeFinal, REDUCE><<<grid, block, 0, c->stream>>>(P, K, A, R); break;
+    case kModeP2GOnly: return launch_one<Pol, TX, TY, kModeP2GOnly>(c, ntiles, P, K, A, R);
+    case kModeFull: return launch_one<Pol, TX, TY, kModeFull>(c, ntiles, P, K, A, R);
+    default: return launch_one<Pol, TX, TY, kModeFinal>(c, ntiles, P, K, A, R);
     }
-    ICM_LAUNCHED("k_tile_substep");
-    return ICM_OK;
 }
 
 template <class Pol>
@@ -345,10 +417,10 @@ static int launch_variant(icm_ctx *c, int mode, int ntiles, const icy_SimParams 
                           const typename Pol::Parts &A, const TileRun &R)
 {
     switch (c->tile_variant) {
-    case 0: return launch_tile<Pol, 16, 8, true>(c, mode, ntiles, P, K, A, R);
-    case 1: return launch_tile<Pol, 16, 16, true>(c, mode, ntiles, P, K, A, R);
-    case 2: return launch_tile<Pol, 32, 8, true>(c, mode, ntiles, P, K, A, R);
-    default: return launch_tile<Pol, 32, 16, true>(c, mode, ntiles, P, K, A, R);
+    case 0: return launch_tile<Pol, 16, 8>(c, mode, ntiles, P, K, A, R);
+    case 1: return launch_tile<Pol, 16, 16>(c, mode, ntiles, P, K, A, R);
+    case 2: return launch_tile<Pol, 32, 8>(c, mode, ntiles, P, K, A, R);
+    default: return launch_tile<Pol, 32, 16>(c, mode, ntiles, P, K, A, R);
     }
 }
 
@@ -384,6 +456,9 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     R.bins = c->d_bins;
     R.err = c->d_err;
     R.fp64_redo = c->d_redo;
+    R.cell_start = c->bin.cell_start;
+    R.group_base = c->bin.group_base;
+    R.strays = c->d_strays;
     R.ind_y = p->indenter_y;
 
     const Consts32 K32 = make_consts32(P);
@@ -488,12 +563,14 @@ extern "C" int icm_create(icm_ctx **out, int device)
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ev_start) != cudaSuccess || cudaEventCreate(&c->ev_stop) != cudaSuccess ||
         cudaMalloc((void **)&c->d_err, sizeof(int)) != cudaSuccess ||
-        cudaMalloc((void **)&c->d_redo, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaMalloc((void **)&c->d_redo, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc((void **)&c->d_strays, sizeof(unsigned long long)) != cudaSuccess) {
         icm_destroy(c);
         return icm::fail(ICM_ERR_CUDA, "icm_create: stream/event/allocation failed");
     }
     cudaMemset(c->d_err, 0, sizeof(int));
     cudaMemset(c->d_redo, 0, sizeof(unsigned long long));
+    cudaMemset(c->d_strays, 0, sizeof(unsigned long long));
     *out = c;
     return ICM_OK;
 }
@@ -505,7 +582,7 @@ extern "C" int icm_destroy(icm_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_fused(c);
     free_binning(c);
-    dfree(c->d_pts); dfree(c->d_grid); dfree(c->d_bins); dfree(c->d_err); dfree(c->d_hist); dfree(c->d_redo);
+    dfree(c->d_pts); dfree(c->d_grid); dfree(c->d_bins); dfree(c->d_err); dfree(c->d_hist); dfree(c->d_redo); dfree(c->d_strays);
     for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
     if (c->ev_start) cudaEventDestroy(c->ev_start);
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
@@ -738,6 +815,14 @@ extern "C" int icm_fp64_redo_count(icm_ctx *c, unsigned long long *out)
 {
     if (!c || !out) return icm::fail(ICM_ERR_ARG, "null argument");
     ICM_CUDA(cudaMemcpyAsync(out, c->d_redo, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    return ICM_OK;
+}
+
+extern "C" int icm_stray_count(icm_ctx *c, unsigned long long *out)
+{
+    if (!c || !out) return icm::fail(ICM_ERR_ARG, "null argument");
+    ICM_CUDA(cudaMemcpyAsync(out, c->d_strays, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     ICM_CUDA(cudaStreamSynchronize(c->stream));
     return ICM_OK;
 }

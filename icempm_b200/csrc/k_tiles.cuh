@@ -1,10 +1,14 @@
 // k_tiles.cuh -- the fused substep: grid update + G2P + P2G in ONE launch.
 //
 // Data layout in HBM (internal, "tile order"):
-//   * particles are binned by the node tile (TX x TY grid nodes) that holds
-//     their stencil base node (int)(x/h - 0.5) and, inside a tile, sorted by
-//     base node; every array is a dense structure-of-arrays in that order, so
-//     a warp reads 32 consecutive particles with one vector load per field;
+//   * particles are binned by their stencil base node (int)(x/h - 0.5); base
+//     nodes (cells) are keyed tile by tile (TX x TY nodes per tile, row-major
+//     inside), and every 32 consecutive keys form a group. Each field is a
+//     structure-of-arrays in ELL slot order: particle r of the cell at lane
+//     L of a group is slot group_base + 32 r + L, with as many rounds as the
+//     group's fullest cell (interior cells of the 4-per-cell lattice hold 4),
+//     so a warp reads one particle of each of its 32 cells per coalesced
+//     vector load;
 //   * the grid is three full-size node buffers G[0..2] of {m, px, py, -};
 //     substep s reads G[s%3] (P2G result of substep s-1), scatters into
 //     G[(s+1)%3] and zeroes G[(s+2)%3] (read by substep s-1), so no separate
@@ -21,16 +25,23 @@
 //      adds its reaction force, reduced in shared memory in FP64;
 //   3. per particle G2P (v2_kernel_g2p, :294-379) from the shared velocities,
 //      advection, Fe update, constitutive model, store;
-//   4. P2G (v2_kernel_p2g, :148-213) of the updated particle for substep s+1
-//      into a shared accumulation region, with a segmented warp-shuffle
-//      reduction over lanes that share a base node before the shared
-//      atomics; particles whose stencil leaves the region fall back to global
-//      atomics;
-//   5. the shared region is added to G[(s+1)%3] with one vector atomic per
-//      touched node (red.global.add.v4.f32 in FP32) and the touched tiles are
-//      flagged dirty.
+//   4. P2G (v2_kernel_p2g, :148-213) of the updated particle for substep s+1.
+//      Particles are walked cell by cell, one lane per cell, so the P2G sums
+//      of a cell (all its particles share the 3x3 stencil) stay in registers
+//      and reach the warp's shared region in 9 conflict-free steps; particles
+//      whose stencil leaves the region fall back to global atomics;
+//   5. the warps' shared regions are added to G[(s+1)%3] with one vector
+//      atomic per touched node (red.global.add.v4.f32 in FP32) and the
+//      touched tiles are flagged dirty.
 // Velocity v and affine matrix Bp never leave registers between substeps;
 // they are written only by the final launch of a run.
+//
+// The weighted sums of G2P and P2G are evaluated column by column (the
+// quadratic B-spline weight is a product wx_i wy_j): G2P forms
+// a_i = sum_j wy_j v_ij and b_i = sum_j wy_j (j - fy) v_ij, then
+// v = sum_i wx_i a_i, Bp = 4/h sum_i [wx_i (i - fx) a_i, wx_i b_i]; P2G
+// writes W_ij (m, c + S_h (i, j)^T) with S_h = h S and
+// c = m v - S_h (fx, fy)^T, which equals W_ij (m, m v + S dpos_ij).
 #pragma once
 #include <cstdint>
 #include "mpm_math32.cuh"
@@ -41,6 +52,19 @@ enum { kModeP2GOnly = 0, kModeFull = 1, kModeFinal = 2 };
 constexpr int kMaxBins = 256;
 
 struct alignas(16) Node64 { double m, px, py, pad; };
+
+// Shared-memory P2G accumulator of one node (one private copy per warp).
+struct Acc64 { double m, px, py; };
+__device__ __forceinline__ void acc_zero(float4 &a) { a = make_float4(0.f, 0.f, 0.f, 0.f); }
+__device__ __forceinline__ void acc_zero(Acc64 &a) { a = Acc64{0, 0, 0}; }
+__device__ __forceinline__ void acc_add(float4 &a, float m, float x, float y) { a.x += m; a.y += x; a.z += y; }
+__device__ __forceinline__ void acc_add(Acc64 &a, double m, double x, double y) { a.m += m; a.px += x; a.py += y; }
+__device__ __forceinline__ float acc_m(const float4 &a) { return a.x; }
+__device__ __forceinline__ float acc_x(const float4 &a) { return a.y; }
+__device__ __forceinline__ float acc_y(const float4 &a) { return a.z; }
+__device__ __forceinline__ double acc_m(const Acc64 &a) { return a.m; }
+__device__ __forceinline__ double acc_x(const Acc64 &a) { return a.px; }
+__device__ __forceinline__ double acc_y(const Acc64 &a) { return a.py; }
 
 struct TileRun {
     int ntx, nty;
@@ -54,26 +78,37 @@ struct TileRun {
     int *err;
     int record_pq;
     unsigned long long *fp64_redo;
+    const int *cell_start;          // binning: cell key k holds cell_start[k+1] - cell_start[k] particles
+    const int *group_base;          // first slot of each group of 32 consecutive cell keys
+    unsigned long long *strays;     // particles that left their binned cell (count)
 };
 
 struct Parts64 { double2 *pos; double4 *F; double *Jp; uint32_t *meta; double2 *vel; double4 *Bp; double2 *pq; };
 struct Parts32 { uint32_t *cell; float2 *frac; float4 *H; float *Jp; uint32_t *meta; float2 *vel; float4 *Bp; float2 *pq; };
 
-__device__ __forceinline__ uint32_t pack_cell(int ix, int iy) { return (uint32_t)(uint16_t)(int16_t)ix | ((uint32_t)(uint16_t)(int16_t)iy << 16); }
+__host__ __device__ __forceinline__ uint32_t pack_cell(int ix, int iy) { return (uint32_t)(uint16_t)(int16_t)ix | ((uint32_t)(uint16_t)(int16_t)iy << 16); }
 __device__ __forceinline__ int cell_x(uint32_t c) { return (int)(int16_t)(uint16_t)(c & 0xffffu); }
 __device__ __forceinline__ int cell_y(uint32_t c) { return (int)(int16_t)(uint16_t)(c >> 16); }
 
+// Symmetric Kirchhoff stress as the P2G needs it.
+template <class T> struct Tau { T t00, t01, t10, t11; };
+
 // ---------------------------------------------------------------- policies
 
-// FP64 reference form: absolute positions, Fe, Jp_inv in double.
+// FP64 reference form: absolute positions, Fe, Jp_inv in double; meta is
+// the grain id (bits 0-15) and the crushed flag (bits 16-23).
 struct Pol64 {
     using real = double;
+    using V2 = double2;
     using Node = Node64;
+    using Acc = Acc64;
     using Parts = Parts64;
     struct Consts { int dummy; };
+    struct Tables { int dummy; };
     struct St { double x, y; M2d F; double Jp; uint32_t meta; };
     struct Sten { int bx, by; double fx, fy, wx[3], wy[3]; };
 
+    static __device__ __forceinline__ void init_tables(Tables &, const Consts &, int, int) {}
     static __device__ __forceinline__ Sten stencil(const icy_SimParams &P, const Consts &, const St &s)
     {
         Stencil64 t = stencil64(s.x, s.y, P.cellsize_inv);
@@ -96,16 +131,23 @@ struct Pol64 {
     }
     static __device__ __forceinline__ void node_velocity(const icy_SimParams &P, const Consts &, const Node &n, int gx,
                                                          int gy, double ix, double iy, double &v0, double &v1,
-                                                         double &f0, double &f1, int &bin)
+                                                         double &f0, double &f1, int &bin, bool contact)
     {
         bin = -1;
         if (n.m == 0) { v0 = 0; v1 = 0; return; }
-        NodeOut o = update_node64(P, gx, gy, n.m, n.px, n.py, ix, iy);
+        NodeOut o = update_node64(P, gx, gy, n.m, n.px, n.py, contact ? ix : 1e300, iy);
         v0 = o.v0; v1 = o.v1; f0 = o.f0; f1 = o.f1; bin = o.bin;
     }
-    // G2P tail: advect, Fe update, constitutive model.
-    static __device__ __forceinline__ void advance(const icy_SimParams &P, const Consts &, St &s, double v0, double v1,
-                                                   const double B[4], double &p_tr, double &q_tr, int &redo)
+    static __device__ __forceinline__ Tau<double> stress(const icy_SimParams &P, const Consts &, const St &s)
+    {
+        M2d t = kirchhoff64(s.F, P.mu, P.kappa);
+        return {t.a00, t.a01, t.a10, t.a11};
+    }
+    // G2P tail: advect, Fe update, constitutive model; returns the stress of
+    // the new Fe for the P2G that follows.
+    static __device__ __forceinline__ Tau<double> advance(const icy_SimParams &P, const Consts &K, const Tables &, St &s,
+                                                          double v0, double v1, const double B[4], double &p_tr,
+                                                          double &q_tr, int &redo)
     {
         const double dt = P.InitialTimeStep;
         s.x += v0 * dt;
@@ -117,40 +159,41 @@ struct Pol64 {
         constitutive64(P, s.F, s.Jp, cr, (int)(int16_t)(s.meta & 0xffffu), p_tr, q_tr);
         s.meta = (s.meta & 0xffffu) | ((uint32_t)cr << 16);
         redo = 0;
+        return stress(P, K, s);
     }
-    static __device__ __forceinline__ void store(const Parts &A, int p, const St &s, const St &old)
+    static __device__ __forceinline__ void store(const Parts &A, int p, const St &s, double jp_old, uint32_t meta_old)
     {
         A.pos[p] = make_double2(s.x, s.y);
         A.F[p] = make_double4(s.F.a00, s.F.a01, s.F.a10, s.F.a11);
-        if (s.Jp != old.Jp) A.Jp[p] = s.Jp;
-        if (s.meta != old.meta) A.meta[p] = s.meta;
-    }
-    // stress impulse of P2G: S = m Bp - dt Vp Dinv tau
-    static __device__ __forceinline__ void p2g_matrix(const icy_SimParams &P, const Consts &, const St &s, const double B[4],
-                                                      double S[4])
-    {
-        M2d tau = kirchhoff64(s.F, P.mu, P.kappa);
-        const double m = P.ParticleMass;
-        double c = (P.InitialTimeStep * P.ParticleVolume) * P.Dp_inv;
-        S[0] = m * B[0] - c * tau.a00;
-        S[1] = m * B[1] - c * tau.a01;
-        S[2] = m * B[2] - c * tau.a10;
-        S[3] = m * B[3] - c * tau.a11;
+        if (s.Jp != jp_old) A.Jp[p] = s.Jp;
+        if (s.meta != meta_old) A.meta[p] = s.meta;
     }
     static __device__ __forceinline__ double mass(const icy_SimParams &P, const Consts &) { return P.ParticleMass; }
     static __device__ __forceinline__ double h(const icy_SimParams &P, const Consts &) { return P.cellsize; }
     static __device__ __forceinline__ double four_h_inv(const icy_SimParams &P, const Consts &) { return 4. * P.cellsize_inv; }
+    static __device__ __forceinline__ double stress_c(const icy_SimParams &P, const Consts &)
+    {
+        return (P.InitialTimeStep * P.ParticleVolume) * P.Dp_inv;
+    }
 };
 
-// FP32 strain form: position = int16 cell + FP32 fraction, H = Fe - I.
+// FP32 strain form: position = int16 cell + FP32 fraction, H = Fe - I; meta
+// holds the grain's residues and the crushed flag (grain_meta32).
 struct Pol32 {
     using real = float;
+    using V2 = float2;
     using Node = float4;
+    using Acc = float4;
     using Parts = Parts32;
     using Consts = Consts32;
+    using Tables = GrainTables32;
     struct St { int ix, iy; float fx, fy; M2f H; float Jp; uint32_t meta; };
     struct Sten { int bx, by; float fx, fy, wx[3], wy[3]; };
 
+    static __device__ __forceinline__ void init_tables(Tables &T, const Consts &K, int tid, int nthr)
+    {
+        grain_tables32_init(T, K, tid, nthr);
+    }
     static __device__ __forceinline__ void base_of(int ic, float f, int &b, float &fr)
     {
         // reference: b = (int)(X - 0.5) (truncation), fr = X - b
@@ -189,38 +232,45 @@ struct Pol32 {
     }
     static __device__ __forceinline__ void node_velocity(const icy_SimParams &P, const Consts &k, const Node &n, int gx,
                                                          int gy, double ind_x, double ind_y, float &v0, float &v1,
-                                                         double &f0, double &f1, int &bin)
+                                                         double &f0, double &f1, int &bin, bool contact)
     {
         bin = -1;
         if (n.x == 0.0f) { v0 = 0.0f; v1 = 0.0f; return; }
-        float a = n.y / n.x, b = n.z / n.x;
-        b -= k.dt * (float)P.Gravity;
-        float vmax = 0.5f * k.h / k.dt;
-        float nrm = sqrtf(a * a + b * b);
-        if (nrm > vmax) { a = a / nrm * vmax; b = b / nrm * vmax; }
-        // contact geometry and reaction in FP64
-        double n0 = gx * P.cellsize - ind_x, n1 = gy * P.cellsize - ind_y;
-        if (n0 * n0 + n1 * n1 < P.IndRSq) {
-            const double vco0 = P.IndVelocity;
-            double va = a, vb = b;
-            double vr0 = va - vco0, vr1 = vb;
-            double z = n0 * n0 + n1 * n1;
-            if (z > 0) { double nn = sqrt(z); n0 /= nn; n1 /= nn; }
-            double vn = vr0 * n0 + vr1 * n1;
-            if (vn < 0) {
-                double vt0 = vr0 - n0 * vn, vt1 = vr1 - n1 * vn;
-                double w0 = vco0 + vt0, w1 = vt1;
-                double mass = n.x;
-                f0 = (va - w0) * mass / P.InitialTimeStep;
-                f1 = (vb - w1) * mass / P.InitialTimeStep;
-                double angle = atan2(n0, n1) + ICM_PI;
-                angle *= P.n_indenter_subdivisions / (2 * ICM_PI);
-                int index = (int)angle;
-                index = max(index, 0);
-                index = min(index, P.n_indenter_subdivisions - 1);
-                bin = index;
-                a = (float)w0;
-                b = (float)w1;
+        float inv_m = 1.0f / n.x;
+        float a = n.y * inv_m, b = n.z * inv_m;
+        b -= k.dt_g;
+        float n2 = a * a + b * b;
+        if (n2 > k.vmax * k.vmax) {
+            float sc = k.vmax * rsqrtf(n2);
+            a *= sc;
+            b *= sc;
+        }
+        // contact geometry and reaction in FP64, only where the CTA's region
+        // can reach the cylinder
+        if (contact) {
+            double n0 = gx * P.cellsize - ind_x, n1 = gy * P.cellsize - ind_y;
+            if (n0 * n0 + n1 * n1 < P.IndRSq) {
+                const double vco0 = P.IndVelocity;
+                double va = a, vb = b;
+                double vr0 = va - vco0, vr1 = vb;
+                double z = n0 * n0 + n1 * n1;
+                if (z > 0) { double nn = sqrt(z); n0 /= nn; n1 /= nn; }
+                double vn = vr0 * n0 + vr1 * n1;
+                if (vn < 0) {
+                    double vt0 = vr0 - n0 * vn, vt1 = vr1 - n1 * vn;
+                    double w0 = vco0 + vt0, w1 = vt1;
+                    double mass = n.x;
+                    f0 = (va - w0) * mass / P.InitialTimeStep;
+                    f1 = (vb - w1) * mass / P.InitialTimeStep;
+                    double angle = atan2(n0, n1) + ICM_PI;
+                    angle *= P.n_indenter_subdivisions / (2 * ICM_PI);
+                    int index = (int)angle;
+                    index = max(index, 0);
+                    index = min(index, P.n_indenter_subdivisions - 1);
+                    bin = index;
+                    a = (float)w0;
+                    b = (float)w1;
+                }
             }
         }
         if (gy <= 2) { a = 0.0f; b = 0.0f; }
@@ -229,8 +279,14 @@ struct Pol32 {
         else if (gx >= P.GridX - 3 && a > 0.0f) a = 0.0f;
         v0 = a; v1 = b;
     }
-    static __device__ __forceinline__ void advance(const icy_SimParams &P, const Consts &k, St &s, float v0, float v1,
-                                                   const float B[4], float &p_tr, float &q_tr, int &redo)
+    static __device__ __forceinline__ Tau<float> stress(const icy_SimParams &, const Consts &k, const St &s)
+    {
+        Tau32 t = tau32(invariants32(s.H, k.mu, k.kappa));
+        return {t.t00, t.t01, t.t01, t.t11};
+    }
+    static __device__ __forceinline__ Tau<float> advance(const icy_SimParams &P, const Consts &k, const Tables &T,
+                                                         St &s, float v0, float v1, const float B[4], float &p_tr,
+                                                         float &q_tr, int &redo)
     {
         // position: fraction inside the cell, renormalised to [0, 1)
         float fx = s.fx + v0 * k.dt_h_inv, fy = s.fy + v1 * k.dt_h_inv;
@@ -247,35 +303,27 @@ struct Pol32 {
         s.H.a01 = H.a01 + (c01 + (c00 * H.a01 + c01 * H.a11));
         s.H.a10 = H.a10 + (c10 + (c10 * H.a00 + c11 * H.a10));
         s.H.a11 = H.a11 + (c11 + (c10 * H.a01 + c11 * H.a11));
-        uint8_t cr = (uint8_t)(s.meta >> 16);
-        int grain = (int)(int16_t)(s.meta & 0xffffu);
         redo = 0;
-        if (constitutive32(k, s.H, s.Jp, cr, grain, p_tr, q_tr) == kC32_NEEDS_FP64) {
-            constitutive32_via64(P, s.H, s.Jp, cr, grain, p_tr, q_tr);
+        Tau32 t;
+        if (constitutive32(k, T, s.H, s.Jp, s.meta, p_tr, q_tr, t) == kC32_NEEDS_FP64) {
+            constitutive32_via64(P, s.H, s.Jp, s.meta, p_tr, q_tr);
             redo = 1;
+            return stress(P, k, s);
         }
-        s.meta = (s.meta & 0xffffu) | ((uint32_t)cr << 16);
+        return {t.t00, t.t01, t.t01, t.t11};
     }
-    static __device__ __forceinline__ void store(const Parts &A, int p, const St &s, const St &old)
+    static __device__ __forceinline__ void store(const Parts &A, int p, const St &s, float jp_old, uint32_t meta_old)
     {
         A.cell[p] = pack_cell(s.ix, s.iy);
         A.frac[p] = make_float2(s.fx, s.fy);
         A.H[p] = make_float4(s.H.a00, s.H.a01, s.H.a10, s.H.a11);
-        if (s.Jp != old.Jp) A.Jp[p] = s.Jp;
-        if (s.meta != old.meta) A.meta[p] = s.meta;
-    }
-    static __device__ __forceinline__ void p2g_matrix(const icy_SimParams &, const Consts &k, const St &s, const float B[4],
-                                                      float S[4])
-    {
-        M2f tau = kirchhoff32(s.H, k.mu, k.kappa);
-        S[0] = k.mass * B[0] - k.stress_c * tau.a00;
-        S[1] = k.mass * B[1] - k.stress_c * tau.a01;
-        S[2] = k.mass * B[2] - k.stress_c * tau.a10;
-        S[3] = k.mass * B[3] - k.stress_c * tau.a11;
+        if (s.Jp != jp_old) A.Jp[p] = s.Jp;
+        if (s.meta != meta_old) A.meta[p] = s.meta;
     }
     static __device__ __forceinline__ float mass(const icy_SimParams &, const Consts &k) { return k.mass; }
     static __device__ __forceinline__ float h(const icy_SimParams &, const Consts &k) { return k.h; }
     static __device__ __forceinline__ float four_h_inv(const icy_SimParams &, const Consts &k) { return k.four_h_inv; }
+    static __device__ __forceinline__ float stress_c(const icy_SimParams &, const Consts &k) { return k.stress_c; }
 };
 
 // ------------------------------------------------------- grid node access
@@ -294,49 +342,62 @@ __device__ __forceinline__ void node_add_global(float4 *g, size_t i, float m, fl
     atomicAdd(&g[i], make_float4(m, px, py, 0.0f));  // red.global.add.v4.f32 (sm_90+)
 }
 
-// ---------------------------------------------------- warp pre-reduction
-
-// Sums a, b, c over runs of consecutive lanes with equal key; the first lane
-// of each run ends up holding the run's totals. Returns true for run heads.
-template <int N, class T>
-__device__ __forceinline__ bool warp_segment_sum(int key, T (&a)[N], T (&b)[N], T (&c)[N])
-{
-    const unsigned FULL = 0xffffffffu;
-    int lane = threadIdx.x & 31;
-    int prev = __shfl_up_sync(FULL, key, 1);
-    bool head = (lane == 0) || (prev != key);
-    unsigned heads = __ballot_sync(FULL, head);
-    unsigned above = (lane == 31) ? 0u : (heads & (0xffffffffu << (lane + 1)));
-    int seg_end = above ? (__ffs(above) - 1) : 32;
-    int len = head ? (seg_end - lane) : 0;
-    int maxlen = __reduce_max_sync(FULL, len);
-    for (int o = 1; o < maxlen; o <<= 1) {
-        bool take = (lane + o) < seg_end;
-#pragma unroll
-        for (int k = 0; k < N; k++) {
-            T oa = __shfl_down_sync(FULL, a[k], o);
-            T ob = __shfl_down_sync(FULL, b[k], o);
-            T oc = __shfl_down_sync(FULL, c[k], o);
-            if (take) { a[k] += oa; b[k] += ob; c[k] += oc; }
-        }
-    }
-    return head;
-}
-
 // ------------------------------------------------------------ the kernel
 
-template <class Pol, int TX, int TY, int MODE, bool REDUCE>
-__global__ void __launch_bounds__(256) k_tile_substep(const icy_SimParams P, const typename Pol::Consts K,
+// Rare paths kept out of line so the hot loop stays small in the
+// instruction cache: the velocity of a node outside the CTA's shared region
+// (recomputed from the scatter buffer) and a scatter into global memory.
+template <class T> struct Pair { T a, b; };
+
+template <class Pol>
+__device__ __noinline__ Pair<typename Pol::real> far_node_velocity(const icy_SimParams &P, const typename Pol::Consts &K,
+                                                                   const typename Pol::Node *g, int gx, int gy,
+                                                                   double ind_x, double ind_y)
+{
+    Pair<typename Pol::real> v{0, 0};
+    if (gx < 0 || gy < 0 || gx >= P.GridX || gy >= P.GridY) return v;
+    double f0, f1;
+    int bin;
+    Pol::node_velocity(P, K, g[(size_t)gy * P.GridX + gx], gx, gy, ind_x, ind_y, v.a, v.b, f0, f1, bin, true);
+    return v;
+}
+
+template <class Pol, int TX, int TY>
+__device__ __noinline__ int far_scatter(const int GX, const int GY, typename Pol::Node *g, uint8_t *dirty, int ntx,
+                                        int gx, int by, typename Pol::real m0, typename Pol::real m1,
+                                        typename Pol::real m2, typename Pol::real x0, typename Pol::real x1,
+                                        typename Pol::real x2, typename Pol::real y0, typename Pol::real y1,
+                                        typename Pol::real y2)
+{
+    const typename Pol::real cm[3] = {m0, m1, m2}, cx[3] = {x0, x1, x2}, cy[3] = {y0, y1, y2};
+    int bad = 0;
+    for (int j = 0; j < 3; j++) {
+        int gy = by + j;
+        if (gx < 0 || gy < 0 || gx >= GX || gy >= GY) { bad = 1; continue; }
+        node_add_global(g, (size_t)gy * GX + gx, cm[j], cx[j], cy[j]);
+        dirty[(gy / TY) * ntx + gx / TX] = 1;
+    }
+    return bad;
+}
+
+template <class Pol, int TX, int TY, int MODE>
+__global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ icy_SimParams P,
+                                                      const __grid_constant__ typename Pol::Consts K,
                                                       const typename Pol::Parts A, const TileRun R)
 {
     using real = typename Pol::real;
+    using V2 = typename Pol::V2;
     using Node = typename Pol::Node;
+    using Acc = typename Pol::Acc;
     constexpr int RX = TX + 4, RY = TY + 4, RN = RX * RY;
-    __shared__ real s_v0[RN], s_v1[RN];
-    __shared__ real s_am[RN], s_ax[RN], s_ay[RN];
+    __shared__ V2 s_v[RN];
+    // one private accumulation region per warp (dynamic shared memory)
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    Acc *s_acc = reinterpret_cast<Acc *>(s_dyn);
     __shared__ double s_bins[2 * kMaxBins];
     __shared__ double s_tot[2];
     __shared__ int s_contact, s_mark[9];
+    __shared__ typename Pol::Tables s_tab;
 
     const int t = blockIdx.x;
     const int tx = t % R.ntx, ty = t / R.ntx;
@@ -379,34 +440,55 @@ __global__ void __launch_bounds__(256) k_tile_substep(const icy_SimParams P, con
         }
     }
     if (tid < 9) s_mark[tid] = 0;
+    if (np > 0 && MODE != kModeP2GOnly) Pol::init_tables(s_tab, K, tid, nthr);
 
     // 2. grid update of the region (velocities into shared memory)
     if (MODE != kModeP2GOnly) {
-        const int nloop = (np > 0) ? RN : TX * TY;
-        for (int k = tid; k < nloop; k += nthr) {
-            int gx, gy;
-            if (np > 0) { gx = rx0 + k % RX; gy = ry0 + k / RX; }
-            else { gx = x0 + k % TX; gy = y0 + k / TX; }
-            real v0 = 0, v1 = 0;
-            if (gx >= 0 && gy >= 0 && gx < GX && gy < GY) {
-                Node n = gA[(size_t)gy * GX + gx];
-                double f0 = 0, f1 = 0;
-                int bin;
-                Pol::node_velocity(P, K, n, gx, gy, R.ind_x, R.ind_y, v0, v1, f0, f1, bin);
-                bool own = gx >= x0 && gx < x0 + TX && gy >= y0 && gy < y0 + TY;
-                if (bin >= 0 && own) {
-                    atomicAdd(&s_bins[2 * bin], f0);
-                    atomicAdd(&s_bins[2 * bin + 1], f1);
-                    atomicAdd(&s_tot[0], f0);
-                    atomicAdd(&s_tot[1], f1);
-                    s_contact = 1;
+        if (np > 0) {
+            for (int k = tid; k < RN; k += nthr) {
+                const int gx = rx0 + k % RX, gy = ry0 + k / RX;
+                real v0 = 0, v1 = 0;
+                if (gx >= 0 && gy >= 0 && gx < GX && gy < GY) {
+                    Node n = gA[(size_t)gy * GX + gx];
+                    double f0 = 0, f1 = 0;
+                    int bin;
+                    Pol::node_velocity(P, K, n, gx, gy, R.ind_x, R.ind_y, v0, v1, f0, f1, bin, contact_possible);
+                    bool own = gx >= x0 && gx < x0 + TX && gy >= y0 && gy < y0 + TY;
+                    if (bin >= 0 && own) {
+                        atomicAdd(&s_bins[2 * bin], f0);
+                        atomicAdd(&s_bins[2 * bin + 1], f1);
+                        atomicAdd(&s_tot[0], f0);
+                        atomicAdd(&s_tot[1], f1);
+                        s_contact = 1;
+                    }
+                }
+                s_v[k].x = v0;
+                s_v[k].y = v1;
+            }
+        } else if (contact_possible) {
+            // no particles here: only the reaction of this tile's own nodes
+            for (int k = tid; k < TX * TY; k += nthr) {
+                const int gx = x0 + k % TX, gy = y0 + k / TX;
+                if (gx < GX && gy < GY) {
+                    Node n = gA[(size_t)gy * GX + gx];
+                    real v0, v1;
+                    double f0 = 0, f1 = 0;
+                    int bin;
+                    Pol::node_velocity(P, K, n, gx, gy, R.ind_x, R.ind_y, v0, v1, f0, f1, bin, true);
+                    if (bin >= 0) {
+                        atomicAdd(&s_bins[2 * bin], f0);
+                        atomicAdd(&s_bins[2 * bin + 1], f1);
+                        atomicAdd(&s_tot[0], f0);
+                        atomicAdd(&s_tot[1], f1);
+                        s_contact = 1;
+                    }
                 }
             }
-            if (np > 0) { s_v0[k] = v0; s_v1[k] = v1; }
         }
     }
+    const int nwarps_blk = nthr >> 5;
     if (MODE != kModeFinal)
-        for (int k = tid; k < RN; k += nthr) { s_am[k] = 0; s_ax[k] = 0; s_ay[k] = 0; }
+        for (int k = tid; k < RN * nwarps_blk; k += nthr) acc_zero(s_acc[k]);
     __syncthreads();
     if (MODE != kModeP2GOnly && contact_possible && s_contact) {
         for (int k = tid; k < 2 * P.n_indenter_subdivisions; k += nthr)
@@ -418,138 +500,193 @@ __global__ void __launch_bounds__(256) k_tile_substep(const icy_SimParams P, con
     }
     if (np == 0) return;
 
-    // 3.-4. particles
+    // 3.-4. particles, one lane per grid cell. A lane walks the particles
+    // binned to its cell and keeps the cell's 27 P2G sums (mass and momentum
+    // of the 3x3 stencil) in registers; lanes of a warp hold distinct cells,
+    // so the sums leave through 9 plain read-modify-write steps into the
+    // warp's region, one warp barrier after each step (two cells a row apart
+    // reach the same node in different steps). A particle whose base node is
+    // no longer its binned cell (it moved since binning) scatters on its
+    // own: shared atomics inside the region, global atomics beyond it.
+    const unsigned FULL = 0xffffffffu;
     const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
-    const real h = Pol::h(P, K), m = Pol::mass(P, K), fhi = Pol::four_h_inv(P, K);
+    const real h = Pol::h(P, K), m = Pol::mass(P, K), fhi = Pol::four_h_inv(P, K), sc = Pol::stress_c(P, K);
+    constexpr int CELLS = TX * TY;
     int bad = 0;
-    unsigned redo_count = 0;
-    for (int pb = p0 + warp * 32; pb < p1; pb += nwarps * 32) {
-        const int p = pb + lane;
-        const bool act = p < p1;
-        typename Pol::St s;
-        real v0 = 0, v1 = 0, B[4] = {0, 0, 0, 0};
-        if (act) {
-            s = Pol::load(A, p);
-            typename Pol::St old = s;
+    unsigned redo_count = 0, stray_count = 0;
+    Acc *wacc = s_acc + warp * RN;
+    for (int cb = warp * 32; cb < CELLS; cb += nwarps * 32) {
+        const int cl = cb + lane;
+        const int clx = cl % TX, cly = cl / TX;
+        const int cbx = x0 + clx, cby = y0 + cly;  // the cell's base node
+        const int gbase = R.group_base[(t * CELLS + cb) >> 5];
+        const int cnt = R.cell_start[t * CELLS + cl + 1] - R.cell_start[t * CELLS + cl];
+        const int rounds = __reduce_max_sync(FULL, cnt);
+        if (rounds == 0) continue;
+        // a cell whose stencil leaves the grid sends every particle down the
+        // stray path, which raises the error word as v2_kernel_p2g does
+        const bool cell_ok = cbx + 2 < GX && cby + 2 < GY;
+        const int ckey = (cly + 1) * RX + (clx + 1);
+        real am[9], ax[9], ay[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) { am[k] = 0; ax[k] = 0; ay[k] = 0; }
+        for (int r = 0; r < rounds; r++) {
+            if (r >= cnt) continue;
+            const int p = gbase + 32 * r + lane;
+            typename Pol::St s = Pol::load(A, p);
+            real v0 = 0, v1 = 0, B[4] = {0, 0, 0, 0};
+            Tau<real> tau;
             if (MODE == kModeP2GOnly) {
                 auto vv = A.vel[p];
                 auto bb = A.Bp[p];
                 v0 = vv.x; v1 = vv.y;
                 B[0] = bb.x; B[1] = bb.y; B[2] = bb.z; B[3] = bb.w;
+                tau = Pol::stress(P, K, s);
             } else {
+                const auto jp_old = s.Jp;
+                const uint32_t meta_old = s.meta;
                 typename Pol::Sten st = Pol::stencil(P, K, s);
-                int lx = st.bx - rx0, ly = st.by - ry0;
-                bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 && st.by >= 0 &&
-                              st.bx + 2 < GX && st.by + 2 < GY;
+                const int lx = st.bx - rx0, ly = st.by - ry0;
+                const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 && st.by >= 0 &&
+                                    st.bx + 2 < GX && st.by + 2 < GY;
+                real a[3][2], b[3][2];
+                if (inside) {
+                    const int q0 = ly * RX + lx;
 #pragma unroll
-                for (int i = 0; i < 3; i++)
+                    for (int i = 0; i < 3; i++) {
+                        a[i][0] = 0; a[i][1] = 0; b[i][0] = 0; b[i][1] = 0;
 #pragma unroll
-                    for (int j = 0; j < 3; j++) {
-                        real n0, n1;
-                        if (inside) {
-                            int q = (ly + j) * RX + lx + i;
-                            n0 = s_v0[q]; n1 = s_v1[q];
-                        } else {
-                            int gx = st.bx + i, gy = st.by + j;
-                            n0 = 0; n1 = 0;
-                            if (gx >= 0 && gy >= 0 && gx < GX && gy < GY) {
-                                Node n = gA[(size_t)gy * GX + gx];
-                                double f0, f1;
-                                int bin;
-                                Pol::node_velocity(P, K, n, gx, gy, R.ind_x, R.ind_y, n0, n1, f0, f1, bin);
-                            }
+                        for (int j = 0; j < 3; j++) {
+                            const V2 n = s_v[q0 + j * RX + i];
+                            const real wyd = st.wy[j] * ((real)j - st.fy);
+                            a[i][0] += st.wy[j] * n.x;
+                            a[i][1] += st.wy[j] * n.y;
+                            b[i][0] += wyd * n.x;
+                            b[i][1] += wyd * n.y;
                         }
-                        real W = st.wx[i] * st.wy[j];
-                        real d0 = (real)i - st.fx, d1 = (real)j - st.fy;
-                        v0 += W * n0;
-                        v1 += W * n1;
-                        real c = fhi * W;
-                        B[0] += c * (n0 * d0);
-                        B[1] += c * (n0 * d1);
-                        B[2] += c * (n1 * d0);
-                        B[3] += c * (n1 * d1);
                     }
+                } else {
+#pragma unroll 1
+                    for (int i = 0; i < 3; i++) {
+                        a[i][0] = 0; a[i][1] = 0; b[i][0] = 0; b[i][1] = 0;
+                        for (int j = 0; j < 3; j++) {
+                            Pair<real> n = far_node_velocity<Pol>(P, K, gA, st.bx + i, st.by + j, R.ind_x, R.ind_y);
+                            const real wyd = st.wy[j] * ((real)j - st.fy);
+                            a[i][0] += st.wy[j] * n.a;
+                            a[i][1] += st.wy[j] * n.b;
+                            b[i][0] += wyd * n.a;
+                            b[i][1] += wyd * n.b;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    const real wxd = st.wx[i] * ((real)i - st.fx);
+                    v0 += st.wx[i] * a[i][0];
+                    v1 += st.wx[i] * a[i][1];
+                    B[0] += wxd * a[i][0];
+                    B[2] += wxd * a[i][1];
+                    B[1] += st.wx[i] * b[i][0];
+                    B[3] += st.wx[i] * b[i][1];
+                }
+                B[0] *= fhi; B[1] *= fhi; B[2] *= fhi; B[3] *= fhi;
                 real p_tr, q_tr;
                 int redo;
-                Pol::advance(P, K, s, v0, v1, B, p_tr, q_tr, redo);
+                tau = Pol::advance(P, K, s_tab, s, v0, v1, B, p_tr, q_tr, redo);
                 redo_count += redo;
-                Pol::store(A, p, s, old);
+                Pol::store(A, p, s, jp_old, meta_old);
                 if (R.record_pq) A.pq[p] = {p_tr, q_tr};
                 if (MODE == kModeFinal) {
                     A.vel[p] = {v0, v1};
                     A.Bp[p] = {B[0], B[1], B[2], B[3]};
                 }
             }
+            if (MODE == kModeFinal) continue;
+
+            // P2G of the (updated) particle: node (i, j) gets
+            // W_ij (m, c + S_h (i, j)^T) with S = m Bp - dt Vp Dinv tau
+            const typename Pol::Sten st = Pol::stencil(P, K, s);
+            const real S00 = h * (m * B[0] - sc * tau.t00), S01 = h * (m * B[1] - sc * tau.t01);
+            const real S10 = h * (m * B[2] - sc * tau.t10), S11 = h * (m * B[3] - sc * tau.t11);
+            const real c0 = v0 * m - (S00 * st.fx + S01 * st.fy);
+            const real c1 = v1 * m - (S10 * st.fx + S11 * st.fy);
+            if (cell_ok && st.bx == cbx && st.by == cby) {
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
+                    const real wm = st.wx[i] * m;
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        const real W = st.wx[i] * st.wy[j];
+                        am[i * 3 + j] += wm * st.wy[j];
+                        ax[i * 3 + j] += W * (u0 + S01 * (real)j);
+                        ay[i * 3 + j] += W * (u1 + S11 * (real)j);
+                    }
+                }
+            } else {
+                stray_count++;
+                const int lx = st.bx - rx0, ly = st.by - ry0;
+                const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 && st.by >= 0 &&
+                                    st.bx + 2 < GX && st.by + 2 < GY;
+#pragma unroll 1
+                for (int i = 0; i < 3; i++) {
+                    real cm[3], cx[3], cy[3];
+                    const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        const real W = st.wx[i] * st.wy[j];
+                        cm[j] = W * m;
+                        cx[j] = W * (u0 + S01 * (real)j);
+                        cy[j] = W * (u1 + S11 * (real)j);
+                    }
+                    if (inside) {
+#pragma unroll
+                        for (int j = 0; j < 3; j++) {
+                            real *ap = reinterpret_cast<real *>(&wacc[(ly + j) * RX + lx + i]);
+                            atomicAdd(ap + 0, cm[j]);
+                            atomicAdd(ap + 1, cx[j]);
+                            atomicAdd(ap + 2, cy[j]);
+                        }
+                    } else {
+                        bad |= far_scatter<Pol, TX, TY>(GX, GY, gB, R.dirty[R.bufB], R.ntx, st.bx + i, st.by, cm[0],
+                                                        cm[1], cm[2], cx[0], cx[1], cx[2], cy[0], cy[1], cy[2]);
+                    }
+                }
+            }
         }
         if (MODE == kModeFinal) continue;
-
-        // P2G of the (updated) particle
-        real cm[9], cx[9], cy[9];
-        int key = -1 - lane;
-        bool fallback = false;
-        typename Pol::Sten st;
-        if (act) {
-            real S[4];
-            Pol::p2g_matrix(P, K, s, B, S);
-            st = Pol::stencil(P, K, s);
-            real mv0 = v0 * m, mv1 = v1 * m;
+        __syncwarp();
 #pragma unroll
-            for (int i = 0; i < 3; i++)
+        for (int i = 0; i < 3; i++)
 #pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    real W = st.wx[i] * st.wy[j];
-                    real d0 = ((real)i - st.fx) * h, d1 = ((real)j - st.fy) * h;
-                    cm[i * 3 + j] = W * m;
-                    cx[i * 3 + j] = W * (mv0 + (S[0] * d0 + S[1] * d1));
-                    cy[i * 3 + j] = W * (mv1 + (S[2] * d0 + S[3] * d1));
+            for (int j = 0; j < 3; j++) {
+                if (cnt > 0 && cell_ok) {
+                    Acc &ac = wacc[ckey + j * RX + i];
+                    Acc v = ac;
+                    acc_add(v, am[i * 3 + j], ax[i * 3 + j], ay[i * 3 + j]);
+                    ac = v;
                 }
-            int lx = st.bx - rx0, ly = st.by - ry0;
-            if (lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 && st.by >= 0 && st.bx + 2 < GX &&
-                st.by + 2 < GY)
-                key = ly * RX + lx;
-            else
-                fallback = true;
-        } else {
-#pragma unroll
-            for (int k = 0; k < 9; k++) { cm[k] = 0; cx[k] = 0; cy[k] = 0; }
-        }
-        bool head = true;
-        if (REDUCE) head = warp_segment_sum<9>(key, cm, cx, cy);
-        if (key >= 0 && head) {
-#pragma unroll
-            for (int i = 0; i < 3; i++)
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    int q = key + j * RX + i;
-                    atomicAdd(&s_am[q], cm[i * 3 + j]);
-                    atomicAdd(&s_ax[q], cx[i * 3 + j]);
-                    atomicAdd(&s_ay[q], cy[i * 3 + j]);
-                }
-        }
-        if (fallback) {
-#pragma unroll
-            for (int i = 0; i < 3; i++)
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    int gx = st.bx + i, gy = st.by + j;
-                    if (gx < 0 || gy < 0 || gx >= GX || gy >= GY) { bad = 1; continue; }
-                    node_add_global(gB, (size_t)gy * GX + gx, cm[i * 3 + j], cx[i * 3 + j], cy[i * 3 + j]);
-                    R.dirty[R.bufB][(gy / TY) * R.ntx + gx / TX] = 1;
-                }
-        }
+                __syncwarp();
+            }
     }
+    if (stray_count && R.strays) atomicAdd(R.strays, (unsigned long long)stray_count);
     if (bad) *R.err = 1;
     if (redo_count && R.fp64_redo) atomicAdd(R.fp64_redo, (unsigned long long)redo_count);
     if (MODE == kModeFinal) return;
     __syncthreads();
 
-    // 5. add the shared region to the scatter buffer
+    // 5. add the warps' shared regions to the scatter buffer
     for (int k = tid; k < RN; k += nthr) {
-        real mm = s_am[k];
+        Acc sum = s_acc[k];
+        for (int w = 1; w < nwarps_blk; w++) {
+            const Acc &o = s_acc[w * RN + k];
+            acc_add(sum, acc_m(o), acc_x(o), acc_y(o));
+        }
+        real mm = acc_m(sum);
         if (mm == 0) continue;
         int gx = rx0 + k % RX, gy = ry0 + k / RX;
         if (gx < 0 || gy < 0 || gx >= GX || gy >= GY) continue;  // unreachable: such stencils take the fallback
-        node_add_global(gB, (size_t)gy * GX + gx, mm, s_ax[k], s_ay[k]);
+        node_add_global(gB, (size_t)gy * GX + gx, mm, acc_x(sum), acc_y(sum));
         int dtx = gx / TX - tx + 1, dty = gy / TY - ty + 1;
         s_mark[dty * 3 + dtx] = 1;
     }
@@ -692,6 +829,24 @@ __global__ void k_bin_order(int ncells, const int *start, int *perm)
     }
 }
 
+// Slots of each group of 32 consecutive cell keys: 32 x the largest count.
+__global__ void k_group_slots(int ngroups, const int *cell_start, int *group_slots)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroups) return;
+    int mx = 0;
+    for (int l = 0; l < 32; l++) mx = max(mx, cell_start[g * 32 + l + 1] - cell_start[g * 32 + l]);
+    group_slots[g] = 32 * mx;
+}
+
+// Slot of the particle at sorted position q (perm order = key order).
+__device__ __forceinline__ int slot_of(int q, const int *perm, const int *key, const int *cell_start,
+                                       const int *group_base)
+{
+    int k = key[perm[q]];
+    return group_base[k >> 5] + 32 * (q - cell_start[k]) + (k & 31);
+}
+
 __global__ void k_tile_starts(int ntiles, int cells_per_tile, const int *cell_start, int *tile_start)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -705,11 +860,13 @@ __device__ __forceinline__ uint32_t read_meta(const icy_SimParams &P, int i)
     return (uint32_t)gr[i] | ((uint32_t)cr[i] << 16);
 }
 
-__global__ void k_pack64(const icy_SimParams P, const int *perm, int *pid, Parts64 A)
+__global__ void k_pack64(const icy_SimParams P, const int *perm, const int *key, const int *cell_start,
+                         const int *group_base, int *pid, Parts64 A)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= P.nPts) return;
-    int i = perm[k];
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.nPts) return;
+    int i = perm[q];
+    int k = slot_of(q, perm, key, cell_start, group_base);
     const double *pts = P.pts_array;
     const size_t pp = P.nPtsPitch;
     auto row = [&](int r) { return pts[(size_t)r * pp + i]; };
@@ -722,11 +879,12 @@ __global__ void k_pack64(const icy_SimParams P, const int *perm, int *pid, Parts
     A.meta[k] = read_meta(P, i);
 }
 
-__global__ void k_unpack64(const icy_SimParams P, const int *pid, const Parts64 A, int write_pq)
+__global__ void k_unpack64(const icy_SimParams P, int nslots, const int *pid, const Parts64 A, int write_pq)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= P.nPts) return;
+    if (k >= nslots) return;
     int i = pid[k];
+    if (i < 0) return;
     double *pts = P.pts_array;
     const size_t pp = P.nPtsPitch;
     auto row = [&](int r) -> double & { return pts[(size_t)r * pp + i]; };
@@ -745,11 +903,13 @@ __global__ void k_unpack64(const icy_SimParams P, const int *pid, const Parts64 
     }
 }
 
-__global__ void k_pack32(const icy_SimParams P, const int *perm, int *pid, Parts32 A)
+__global__ void k_pack32(const icy_SimParams P, const int *perm, const int *key, const int *cell_start,
+                         const int *group_base, int *pid, Parts32 A)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= P.nPts) return;
-    int i = perm[k];
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= P.nPts) return;
+    int i = perm[q];
+    int k = slot_of(q, perm, key, cell_start, group_base);
     const double *pts = P.pts_array;
     const size_t pp = P.nPtsPitch;
     auto row = [&](int r) { return pts[(size_t)r * pp + i]; };
@@ -768,14 +928,17 @@ __global__ void k_pack32(const icy_SimParams P, const int *perm, int *pid, Parts
     A.Bp[k] = make_float4((float)row(ICM_IDX_BP00), (float)row(ICM_IDX_BP00 + 1), (float)row(ICM_IDX_BP00 + 2),
                           (float)row(ICM_IDX_BP00 + 3));
     A.Jp[k] = (float)row(ICM_IDX_JP_INV);
-    A.meta[k] = read_meta(P, i);
+    const uint8_t *cr = (const uint8_t *)P.pts_array;
+    const int16_t *gr = (const int16_t *)((const char *)P.pts_array + P.nPtsPitch);
+    A.meta[k] = grain_meta32(gr[i], cr[i]);
 }
 
-__global__ void k_unpack32(const icy_SimParams P, const int *pid, const Parts32 A, int write_pq)
+__global__ void k_unpack32(const icy_SimParams P, int nslots, const int *pid, const Parts32 A, int write_pq)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= P.nPts) return;
+    if (k >= nslots) return;
     int i = pid[k];
+    if (i < 0) return;
     double *pts = P.pts_array;
     const size_t pp = P.nPtsPitch;
     auto row = [&](int r) -> double & { return pts[(size_t)r * pp + i]; };
@@ -789,7 +952,7 @@ __global__ void k_unpack32(const icy_SimParams P, const int *pid, const Parts32 
     row(ICM_IDX_FE00 + 2) = H.z; row(ICM_IDX_FE00 + 3) = 1.0 + (double)H.w;
     row(ICM_IDX_BP00) = B.x; row(ICM_IDX_BP00 + 1) = B.y; row(ICM_IDX_BP00 + 2) = B.z; row(ICM_IDX_BP00 + 3) = B.w;
     row(ICM_IDX_JP_INV) = A.Jp[k];
-    ((uint8_t *)pts)[i] = (uint8_t)(A.meta[k] >> 16);
+    ((uint8_t *)pts)[i] = (uint8_t)meta32_crushed(A.meta[k]);
     if (write_pq) {
         float2 q = A.pq[k];
         row(ICM_IDX_P) = q.x;

@@ -102,7 +102,8 @@ int icm_destroy(icm_ctx *ctx);
 int icm_set_form(icm_ctx *ctx, int form);
 int icm_get_form(icm_ctx *ctx);
 /* Tile shape of the fused forms: index into the built variants
- * (0: 16x8, 1: 16x16, 2: 32x8, 3: 32x16 nodes) and block size. */
+ * (0: 16x8, 1: 16x16, 2: 32x8, 3: 32x16 nodes) and block size (default
+ * 16x16 nodes, 128 threads). */
 int icm_set_tile(icm_ctx *ctx, int tile_variant, int threads);
 int icm_get_tile(icm_ctx *ctx, int *tile_variant, int *threads);
 /* GPU_Implementation5::cuda_allocate_arrays (gpu_implementation5.cu:481-513):
@@ -153,6 +154,11 @@ int icm_force_history(icm_ctx *ctx, double *host_out, int n);
 /* Number of particles the FP32 form handed to the FP64 fallback since the
  * context was created (synchronous). */
 int icm_fp64_redo_count(icm_ctx *ctx, unsigned long long *out);
+/* Particle-substeps of the fused forms in which a particle's base node was
+ * no longer the grid cell it was binned to (it then scatters through the
+ * slower per-particle path); cumulative since the context was created
+ * (synchronous). */
+int icm_stray_count(icm_ctx *ctx, unsigned long long *out);
 /* CUDA events around work on the context's stream (eventCycleStart/Stop of
  * gpu_implementation5.h:61). */
 int icm_record_start(icm_ctx *ctx);
