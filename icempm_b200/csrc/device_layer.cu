@@ -389,9 +389,12 @@ static int launch_one(icm_ctx *c, int ntiles, const icy_SimParams &P, const type
                       const typename Pol::Parts &A, const TileRun &R)
 {
     constexpr int RN = (TX + 4) * (TY + 4);
-    const size_t dyn = (MODE == kModeFinal) ? 0 : sizeof(typename Pol::Acc) * RN * (size_t)(c->threads / 32);
+    const int nwarps = c->threads / 32;
+    if (TX * TY > 32 * kMaxGroupsPerWarp * nwarps || nwarps > kMaxWarps)
+        return icm::fail(ICM_ERR_ARG, "tile too large for the block size (need threads >= TX*TY/4)");
+    const size_t dyn = tile_dyn_bytes<Pol, MODE>(RN, nwarps);
     static size_t opted = 0;  // static + dynamic shared memory above 48 KB needs the opt-in
-    if (MODE != kModeFinal && dyn > opted) {
+    if (dyn > opted) {  // also needed when static + dynamic exceed 48 KB
         ICM_CUDA(cudaFuncSetAttribute(k_tile_substep<Pol, TX, TY, MODE>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
         opted = dyn;

@@ -44,12 +44,16 @@
 // c = m v - S_h (fx, fy)^T, which equals W_ij (m, m v + S dpos_ij).
 #pragma once
 #include <cstdint>
+#include <cuda_pipeline.h>
 #include "mpm_math32.cuh"
 
 namespace icm {
 
 enum { kModeP2GOnly = 0, kModeFull = 1, kModeFinal = 2 };
 constexpr int kMaxBins = 256;
+// a CTA has at most 8 warps and each warp at most 4 groups of 32 cells, so
+// a tile of TX*TY cells needs at least TX*TY/128 warps
+constexpr int kMaxWarps = 8, kMaxGroupsPerWarp = 4;
 
 struct alignas(16) Node64 { double m, px, py, pad; };
 
@@ -107,6 +111,28 @@ struct Pol64 {
     struct Tables { int dummy; };
     struct St { double x, y; M2d F; double Jp; uint32_t meta; };
     struct Sten { int bx, by; double fx, fy, wx[3], wy[3]; };
+    // one round of a warp (32 particles) staged in shared memory
+    struct Stage { double4 F[32]; double2 pos[32]; double Jp[32]; uint32_t meta[32]; };
+
+    static __device__ __forceinline__ void prefetch(const Parts &A, int p, Stage &S, int lane)
+    {
+        __pipeline_memcpy_async(&S.F[lane], &A.F[p], 16);
+        __pipeline_memcpy_async(reinterpret_cast<char *>(&S.F[lane]) + 16, reinterpret_cast<const char *>(&A.F[p]) + 16, 16);
+        __pipeline_memcpy_async(&S.pos[lane], &A.pos[p], 16);
+        __pipeline_memcpy_async(&S.Jp[lane], &A.Jp[p], 8);
+        __pipeline_memcpy_async(&S.meta[lane], &A.meta[p], 4);
+    }
+    static __device__ __forceinline__ St load_staged(const Stage &S, int lane)
+    {
+        St s;
+        double2 x = S.pos[lane];
+        double4 F = S.F[lane];
+        s.x = x.x; s.y = x.y;
+        s.F = {F.x, F.y, F.z, F.w};
+        s.Jp = S.Jp[lane];
+        s.meta = S.meta[lane];
+        return s;
+    }
 
     static __device__ __forceinline__ void init_tables(Tables &, const Consts &, int, int) {}
     static __device__ __forceinline__ Sten stencil(const icy_SimParams &P, const Consts &, const St &s)
@@ -189,6 +215,30 @@ struct Pol32 {
     using Tables = GrainTables32;
     struct St { int ix, iy; float fx, fy; M2f H; float Jp; uint32_t meta; };
     struct Sten { int bx, by; float fx, fy, wx[3], wy[3]; };
+    // one round of a warp (32 particles) staged in shared memory
+    struct Stage { float4 H[32]; float2 frac[32]; uint32_t cell[32]; float Jp[32]; uint32_t meta[32]; };
+
+    static __device__ __forceinline__ void prefetch(const Parts &A, int p, Stage &S, int lane)
+    {
+        __pipeline_memcpy_async(&S.H[lane], &A.H[p], 16);
+        __pipeline_memcpy_async(&S.frac[lane], &A.frac[p], 8);
+        __pipeline_memcpy_async(&S.cell[lane], &A.cell[p], 4);
+        __pipeline_memcpy_async(&S.Jp[lane], &A.Jp[p], 4);
+        __pipeline_memcpy_async(&S.meta[lane], &A.meta[p], 4);
+    }
+    static __device__ __forceinline__ St load_staged(const Stage &S, int lane)
+    {
+        St s;
+        uint32_t c = S.cell[lane];
+        float2 f = S.frac[lane];
+        float4 H = S.H[lane];
+        s.ix = cell_x(c); s.iy = cell_y(c);
+        s.fx = f.x; s.fy = f.y;
+        s.H = {H.x, H.y, H.z, H.w};
+        s.Jp = S.Jp[lane];
+        s.meta = S.meta[lane];
+        return s;
+    }
 
     static __device__ __forceinline__ void init_tables(Tables &T, const Consts &K, int tid, int nthr)
     {
@@ -380,6 +430,20 @@ __device__ __noinline__ int far_scatter(const int GX, const int GY, typename Pol
     return bad;
 }
 
+// Dynamic shared memory of one CTA (host and kernel use the same layout):
+// the warps' P2G regions (none in the final launch), then two staging rounds
+// per warp.
+template <class Pol, int MODE>
+__host__ __device__ constexpr size_t tile_region_bytes(int RN, int nwarps)
+{
+    return (MODE == kModeFinal) ? 0 : (size_t)nwarps * RN * sizeof(typename Pol::Acc);
+}
+template <class Pol, int MODE>
+__host__ __device__ constexpr size_t tile_dyn_bytes(int RN, int nwarps)
+{
+    return tile_region_bytes<Pol, MODE>(RN, nwarps) + (size_t)nwarps * 2 * sizeof(typename Pol::Stage);
+}
+
 template <class Pol, int TX, int TY, int MODE>
 __global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ icy_SimParams P,
                                                       const __grid_constant__ typename Pol::Consts K,
@@ -398,6 +462,8 @@ __global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ ic
     __shared__ double s_tot[2];
     __shared__ int s_contact, s_mark[9];
     __shared__ typename Pol::Tables s_tab;
+    __shared__ int s_wcnt[kMaxWarps][kMaxGroupsPerWarp][32];
+    __shared__ int s_wrounds[kMaxWarps][kMaxGroupsPerWarp], s_wgbase[kMaxWarps][kMaxGroupsPerWarp];
 
     const int t = blockIdx.x;
     const int tx = t % R.ntx, ty = t / R.ntx;
@@ -445,25 +511,38 @@ __global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ ic
     // 2. grid update of the region (velocities into shared memory)
     if (MODE != kModeP2GOnly) {
         if (np > 0) {
-            for (int k = tid; k < RN; k += nthr) {
-                const int gx = rx0 + k % RX, gy = ry0 + k / RX;
-                real v0 = 0, v1 = 0;
-                if (gx >= 0 && gy >= 0 && gx < GX && gy < GY) {
-                    Node n = gA[(size_t)gy * GX + gx];
-                    double f0 = 0, f1 = 0;
-                    int bin;
-                    Pol::node_velocity(P, K, n, gx, gy, R.ind_x, R.ind_y, v0, v1, f0, f1, bin, contact_possible);
-                    bool own = gx >= x0 && gx < x0 + TX && gy >= y0 && gy < y0 + TY;
-                    if (bin >= 0 && own) {
-                        atomicAdd(&s_bins[2 * bin], f0);
-                        atomicAdd(&s_bins[2 * bin + 1], f1);
-                        atomicAdd(&s_tot[0], f0);
-                        atomicAdd(&s_tot[1], f1);
-                        s_contact = 1;
-                    }
+            // four nodes per thread per pass: their loads are issued together
+            constexpr int NB = 4;
+            for (int k0 = tid; k0 < RN; k0 += NB * nthr) {
+                Node nd[NB];
+#pragma unroll
+                for (int b = 0; b < NB; b++) {
+                    const int k = k0 + b * nthr;
+                    const int gx = rx0 + k % RX, gy = ry0 + k / RX;
+                    if (k < RN && gx >= 0 && gy >= 0 && gx < GX && gy < GY) nd[b] = gA[(size_t)gy * GX + gx];
                 }
-                s_v[k].x = v0;
-                s_v[k].y = v1;
+#pragma unroll
+                for (int b = 0; b < NB; b++) {
+                    const int k = k0 + b * nthr;
+                    if (k >= RN) break;
+                    const int gx = rx0 + k % RX, gy = ry0 + k / RX;
+                    real v0 = 0, v1 = 0;
+                    if (gx >= 0 && gy >= 0 && gx < GX && gy < GY) {
+                        double f0 = 0, f1 = 0;
+                        int bin;
+                        Pol::node_velocity(P, K, nd[b], gx, gy, R.ind_x, R.ind_y, v0, v1, f0, f1, bin, contact_possible);
+                        bool own = gx >= x0 && gx < x0 + TX && gy >= y0 && gy < y0 + TY;
+                        if (bin >= 0 && own) {
+                            atomicAdd(&s_bins[2 * bin], f0);
+                            atomicAdd(&s_bins[2 * bin + 1], f1);
+                            atomicAdd(&s_tot[0], f0);
+                            atomicAdd(&s_tot[1], f1);
+                            s_contact = 1;
+                        }
+                    }
+                    s_v[k].x = v0;
+                    s_v[k].y = v1;
+                }
             }
         } else if (contact_possible) {
             // no particles here: only the reaction of this tile's own nodes
@@ -512,30 +591,68 @@ __global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ ic
     const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
     const real h = Pol::h(P, K), m = Pol::mass(P, K), fhi = Pol::four_h_inv(P, K), sc = Pol::stress_c(P, K);
     constexpr int CELLS = TX * TY;
+    constexpr int NGT = CELLS / 32;  // groups of 32 cells in the tile
     int bad = 0;
     unsigned redo_count = 0, stray_count = 0;
     Acc *wacc = s_acc + warp * RN;
-    for (int cb = warp * 32; cb < CELLS; cb += nwarps * 32) {
-        const int cl = cb + lane;
+    typename Pol::Stage *stage =
+        reinterpret_cast<typename Pol::Stage *>(s_dyn + tile_region_bytes<Pol, MODE>(RN, nwarps)) + 2 * warp;
+
+    // this warp's groups g = warp, warp + nwarps, ... (at most kMaxGroupsPerWarp)
+    int ng_w = 0;
+    for (int g = warp; g < NGT; g += nwarps, ng_w++) {
+        const int c = t * CELLS + g * 32 + lane;
+        const int cnt = R.cell_start[c + 1] - R.cell_start[c];
+        s_wcnt[warp][ng_w][lane] = cnt;
+        const int rounds = __reduce_max_sync(FULL, cnt);
+        if (lane == 0) {
+            s_wrounds[warp][ng_w] = rounds;
+            s_wgbase[warp][ng_w] = R.group_base[(t * CELLS >> 5) + g];
+        }
+    }
+    __syncwarp();
+    // work items (k, r): round r of the warp's k-th group; the next item's
+    // particle state is copied into the other stage while this one computes
+    auto next_item = [&](int k, int r, int &nk, int &nr) {
+        nk = k;
+        nr = r + 1;
+        if (nr >= s_wrounds[warp][k]) {
+            nr = 0;
+            nk = k + 1;
+            while (nk < ng_w && s_wrounds[warp][nk] == 0) nk++;
+        }
+    };
+    auto issue = [&](int k, int r, int st) {
+        if (k < ng_w && r < s_wcnt[warp][k][lane]) Pol::prefetch(A, s_wgbase[warp][k] + 32 * r + lane, stage[st], lane);
+        __pipeline_commit();
+    };
+    int k = 0, r = 0, cur = 0;
+    while (k < ng_w && s_wrounds[warp][k] == 0) k++;
+    issue(k, 0, 0);
+    real am[9], ax[9], ay[9];
+    while (k < ng_w) {
+        int nk, nr;
+        next_item(k, r, nk, nr);
+        issue(nk, nr, cur ^ 1);
+        __pipeline_wait_prior(1);
+        const int g = warp + k * nwarps;
+        const int cl = g * 32 + lane;
         const int clx = cl % TX, cly = cl / TX;
         const int cbx = x0 + clx, cby = y0 + cly;  // the cell's base node
-        const int gbase = R.group_base[(t * CELLS + cb) >> 5];
-        const int cnt = R.cell_start[t * CELLS + cl + 1] - R.cell_start[t * CELLS + cl];
-        const int rounds = __reduce_max_sync(FULL, cnt);
-        if (rounds == 0) continue;
+        const int cnt = s_wcnt[warp][k][lane];
         // a cell whose stencil leaves the grid sends every particle down the
         // stray path, which raises the error word as v2_kernel_p2g does
         const bool cell_ok = cbx + 2 < GX && cby + 2 < GY;
-        const int ckey = (cly + 1) * RX + (clx + 1);
-        real am[9], ax[9], ay[9];
+        if (r == 0) {
 #pragma unroll
-        for (int k = 0; k < 9; k++) { am[k] = 0; ax[k] = 0; ay[k] = 0; }
-        for (int r = 0; r < rounds; r++) {
-            if (r >= cnt) continue;
-            const int p = gbase + 32 * r + lane;
-            typename Pol::St s = Pol::load(A, p);
+            for (int q = 0; q < 9; q++) { am[q] = 0; ax[q] = 0; ay[q] = 0; }
+        }
+        if (r < cnt) {
+            const int p = s_wgbase[warp][k] + 32 * r + lane;
+            typename Pol::St s = Pol::load_staged(stage[cur], lane);
             real v0 = 0, v1 = 0, B[4] = {0, 0, 0, 0};
             Tau<real> tau;
+            bool do_p2g = MODE != kModeFinal;
             if (MODE == kModeP2GOnly) {
                 auto vv = A.vel[p];
                 auto bb = A.Bp[p];
@@ -601,74 +718,82 @@ __global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ ic
                     A.Bp[p] = {B[0], B[1], B[2], B[3]};
                 }
             }
-            if (MODE == kModeFinal) continue;
-
-            // P2G of the (updated) particle: node (i, j) gets
-            // W_ij (m, c + S_h (i, j)^T) with S = m Bp - dt Vp Dinv tau
-            const typename Pol::Sten st = Pol::stencil(P, K, s);
-            const real S00 = h * (m * B[0] - sc * tau.t00), S01 = h * (m * B[1] - sc * tau.t01);
-            const real S10 = h * (m * B[2] - sc * tau.t10), S11 = h * (m * B[3] - sc * tau.t11);
-            const real c0 = v0 * m - (S00 * st.fx + S01 * st.fy);
-            const real c1 = v1 * m - (S10 * st.fx + S11 * st.fy);
-            if (cell_ok && st.bx == cbx && st.by == cby) {
+            if (do_p2g) {
+                // P2G of the (updated) particle: node (i, j) gets
+                // W_ij (m, c + S_h (i, j)^T) with S = m Bp - dt Vp Dinv tau
+                const typename Pol::Sten st = Pol::stencil(P, K, s);
+                const real S00 = h * (m * B[0] - sc * tau.t00), S01 = h * (m * B[1] - sc * tau.t01);
+                const real S10 = h * (m * B[2] - sc * tau.t10), S11 = h * (m * B[3] - sc * tau.t11);
+                const real c0 = v0 * m - (S00 * st.fx + S01 * st.fy);
+                const real c1 = v1 * m - (S10 * st.fx + S11 * st.fy);
+                if (cell_ok && st.bx == cbx && st.by == cby) {
 #pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
-                    const real wm = st.wx[i] * m;
-#pragma unroll
-                    for (int j = 0; j < 3; j++) {
-                        const real W = st.wx[i] * st.wy[j];
-                        am[i * 3 + j] += wm * st.wy[j];
-                        ax[i * 3 + j] += W * (u0 + S01 * (real)j);
-                        ay[i * 3 + j] += W * (u1 + S11 * (real)j);
-                    }
-                }
-            } else {
-                stray_count++;
-                const int lx = st.bx - rx0, ly = st.by - ry0;
-                const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 && st.by >= 0 &&
-                                    st.bx + 2 < GX && st.by + 2 < GY;
-#pragma unroll 1
-                for (int i = 0; i < 3; i++) {
-                    real cm[3], cx[3], cy[3];
-                    const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
-#pragma unroll
-                    for (int j = 0; j < 3; j++) {
-                        const real W = st.wx[i] * st.wy[j];
-                        cm[j] = W * m;
-                        cx[j] = W * (u0 + S01 * (real)j);
-                        cy[j] = W * (u1 + S11 * (real)j);
-                    }
-                    if (inside) {
+                    for (int i = 0; i < 3; i++) {
+                        const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
+                        const real wm = st.wx[i] * m;
 #pragma unroll
                         for (int j = 0; j < 3; j++) {
-                            real *ap = reinterpret_cast<real *>(&wacc[(ly + j) * RX + lx + i]);
-                            atomicAdd(ap + 0, cm[j]);
-                            atomicAdd(ap + 1, cx[j]);
-                            atomicAdd(ap + 2, cy[j]);
+                            const real W = st.wx[i] * st.wy[j];
+                            am[i * 3 + j] += wm * st.wy[j];
+                            ax[i * 3 + j] += W * (u0 + S01 * (real)j);
+                            ay[i * 3 + j] += W * (u1 + S11 * (real)j);
                         }
-                    } else {
-                        bad |= far_scatter<Pol, TX, TY>(GX, GY, gB, R.dirty[R.bufB], R.ntx, st.bx + i, st.by, cm[0],
-                                                        cm[1], cm[2], cx[0], cx[1], cx[2], cy[0], cy[1], cy[2]);
+                    }
+                } else {
+                    stray_count++;
+                    const int lx = st.bx - rx0, ly = st.by - ry0;
+                    const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 &&
+                                        st.by >= 0 && st.bx + 2 < GX && st.by + 2 < GY;
+#pragma unroll 1
+                    for (int i = 0; i < 3; i++) {
+                        real cm[3], cx[3], cy[3];
+                        const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
+#pragma unroll
+                        for (int j = 0; j < 3; j++) {
+                            const real W = st.wx[i] * st.wy[j];
+                            cm[j] = W * m;
+                            cx[j] = W * (u0 + S01 * (real)j);
+                            cy[j] = W * (u1 + S11 * (real)j);
+                        }
+                        if (inside) {
+#pragma unroll
+                            for (int j = 0; j < 3; j++) {
+                                real *ap = reinterpret_cast<real *>(&wacc[(ly + j) * RX + lx + i]);
+                                atomicAdd(ap + 0, cm[j]);
+                                atomicAdd(ap + 1, cx[j]);
+                                atomicAdd(ap + 2, cy[j]);
+                            }
+                        } else {
+                            bad |= far_scatter<Pol, TX, TY>(GX, GY, gB, R.dirty[R.bufB], R.ntx, st.bx + i, st.by,
+                                                            cm[0], cm[1], cm[2], cx[0], cx[1], cx[2], cy[0], cy[1],
+                                                            cy[2]);
+                        }
                     }
                 }
             }
         }
-        if (MODE == kModeFinal) continue;
-        __syncwarp();
+        // last round of this group: its cells' sums go to the warp's region
+        if (MODE != kModeFinal && nk != k) {
+            const int ckey = (cly + 1) * RX + (clx + 1);
+            __syncwarp();
 #pragma unroll
-        for (int i = 0; i < 3; i++)
+            for (int i = 0; i < 3; i++)
 #pragma unroll
-            for (int j = 0; j < 3; j++) {
-                if (cnt > 0 && cell_ok) {
-                    Acc &ac = wacc[ckey + j * RX + i];
-                    Acc v = ac;
-                    acc_add(v, am[i * 3 + j], ax[i * 3 + j], ay[i * 3 + j]);
-                    ac = v;
+                for (int j = 0; j < 3; j++) {
+                    if (cnt > 0 && cell_ok) {
+                        Acc &ac = wacc[ckey + j * RX + i];
+                        Acc v = ac;
+                        acc_add(v, am[i * 3 + j], ax[i * 3 + j], ay[i * 3 + j]);
+                        ac = v;
+                    }
+                    __syncwarp();
                 }
-                __syncwarp();
-            }
+        }
+        k = nk;
+        r = nr;
+        cur ^= 1;
     }
+    __pipeline_wait_prior(0);
     if (stray_count && R.strays) atomicAdd(R.strays, (unsigned long long)stray_count);
     if (bad) *R.err = 1;
     if (redo_count && R.fp64_redo) atomicAdd(R.fp64_redo, (unsigned long long)redo_count);
