@@ -173,6 +173,24 @@ int icm_kernel_time(icm_ctx *ctx, double *total_ms, long long *launches);
 /* The context's CUDA stream (cudaStream_t) for callers that interleave
  * their own work. */
 void *icm_stream(icm_ctx *ctx);
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory while they run -- an allocation can block or synchronise the whole
+ * device, a host framework may own all GPU memory through its own pool, or
+ * the caller works to a fixed memory budget -- this runs n substeps of the
+ * FP64 step-wise form (the arithmetic of icm_run_substeps with
+ * ICM_FORM_FP64_STEPWISE) on caller-owned device buffers and allocates
+ * nothing: pts is the particle SoA (16 rows x p->nPtsPitch doubles, updated
+ * in place), bins the 2*n_indenter_subdivisions force bins (accumulated),
+ * err the error word (set to 1 when a stencil leaves the grid), stream a
+ * cudaStream_t (NULL: the default stream). p is advanced as by
+ * icm_run_substeps. The grid scratch is a fixed array inside the library:
+ * GridX*GridY may be at most 262,144 nodes (6 MiB, held by every GPU that
+ * loads the library until exit); larger grids are rejected with
+ * ICM_ERR_ARG. All calls share that scratch, so calls that overlap on the
+ * GPU race and must not be issued concurrently. The first call on a device
+ * looks up the scratch's device address; make that first call before any
+ * stream capture. */
+int icm_run_substeps_noalloc(icy_SimParams *p, double *pts, double *bins, int *err, int n, void *stream);
 /* Pinned host memory for transfer buffers (cudaMallocHost/cudaFreeHost). */
 int icm_host_alloc(void **ptr, size_t bytes);
 int icm_host_free(void *ptr);
