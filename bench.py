@@ -243,14 +243,14 @@ def main():
     na = configs.active_nodes(p0, soa0)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
-    def make(form, tile):
+    def make(form, tile, threads=None):
         m = im.Model(local)
         m.prms = configs.make_params(name)
         m.gpu.model = m
         gx, gy, dim, dt, cx, cy, _ = configs.CONFIGS[name]
         m.load_block(cx, cy, 0.2, 0.05, 12345)
         m.gpu.set_form(form)
-        m.gpu.set_tile(tile, args.threads)
+        m.gpu.set_tile(tile, threads or args.threads)
         return m
 
     def timed(m, steps, warmup, substeps, ktime=False, clocks=None):
@@ -311,14 +311,21 @@ def main():
 
     extra = {}
     # --- FP64 forms (the plain drop-in and the fused FP64 form)
+    tile64, threads64 = tile, args.threads
     if not args.no_fp64:
+        if args.tile < 0:
+            from icempm_b200 import autotune
+
+            tile64, threads64, _ = autotune.choose(name, im.FORM_FP64, local)
         k2 = max(2, args.steps // 3)
         for form, key in ((im.FORM_FP64, "fp64_fused"), (im.FORM_FP64_STEPWISE, "fp64_stepwise")):
-            mm = make(form, tile)
+            mm = make(form, tile64, threads64)
             ms2, (k2ms, k2n) = timed(mm, k2, 1, args.substeps, ktime=(form == im.FORM_FP64))
             t2 = max_over_ranks(sum(ms2) / 1e3)
             v2 = world * n * args.substeps * k2 / t2
-            d = {"value": v2, "ms_per_step": sum(ms2) / k2, "steps": k2}
+            d = {"value": v2, "ms_per_step": sum(ms2) / k2, "steps": k2,
+                 "tile": im.TILE_VARIANTS[tile64] if form == im.FORM_FP64 else None,
+                 "threads": threads64 if form == im.FORM_FP64 else None}
             if k2n:
                 a2 = alg_bytes("fp64", n, na, ng) / (k2ms / k2n / 1e3) / 1e9
                 d["roofline"] = {"achieved": a2, "frac": a2 / hbm, "avg_launch_us": 1e3 * k2ms / k2n}
@@ -331,9 +338,12 @@ def main():
     if not args.no_accuracy and rank == 0:
         nsub = configs.CONFIGS[name][6]
         res = {}
-        for form in (im.FORM_FP64, im.FORM_FP32):
-            mm = make(form, tile)
+        strays = {}
+        for form in (im.FORM_FP64, im.FORM_FP32, im.FORM_FP64_STEPWISE):
+            mm = make(form, tile64 if form != im.FORM_FP32 else tile, threads64 if form != im.FORM_FP32 else None)
             mm.gpu.run_substeps(mm.prms, nsub)
+            if form != im.FORM_FP64_STEPWISE:
+                strays[form] = mm.gpu.stray_count()
             hist = mm.gpu.force_history(nsub)
             mm.gpu.cuda_transfer_from_device()
             mm.gpu.synchronize()
@@ -341,8 +351,14 @@ def main():
             mm.gpu.close()
         h64, s64, e64 = res[im.FORM_FP64]
         h32, s32, e32 = res[im.FORM_FP32]
+        hsw, ssw, esw = res[im.FORM_FP64_STEPWISE]
         f64 = np.hypot(h64[:, 0], h64[:, 1])
         f32 = np.hypot(h32[:, 0], h32[:, 1])
+        fsw = np.hypot(hsw[:, 0], hsw[:, 1])
+        win = 100  # substeps per window of the smoothed force history
+
+        def smooth(f):
+            return f[: len(f) // win * win].reshape(-1, win).mean(axis=1)
         pitch = int(p0.nPtsPitch)
         x64 = s64[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n]
         x32 = s32[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n]
@@ -353,8 +369,19 @@ def main():
             "force_history_rel_l2": float(np.linalg.norm(f32 - f64) / max(np.linalg.norm(f64), 1e-30)),
             "max_pos_err_h": float(np.abs(x32 - x64).max() / p0.cellsize),
             "p99_pos_err_h": float(np.percentile(np.abs(x32 - x64).max(axis=0), 99) / p0.cellsize),
-            "error_flags": [int(e64), int(e32)],
+            "peak_force_rel_err_100substep_avg": float(abs(smooth(f32).max() - smooth(f64).max()) /
+                                                       max(smooth(f64).max(), 1e-30)),
+            "frame_impulse_rel_err": float(abs(f32.sum() - f64.sum()) / max(abs(f64.sum()), 1e-30)),
+            "fp64_vs_fp64_stepwise": {
+                "peak_force_rel_err": float(abs(fsw.max() - f64.max()) / max(f64.max(), 1e-30)),
+                "peak_force_rel_err_100substep_avg": float(abs(smooth(fsw).max() - smooth(f64).max()) /
+                                                           max(smooth(f64).max(), 1e-30)),
+                "max_pos_err_h": float(np.abs(ssw[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n] - x64).max() /
+                                       p0.cellsize),
+            },
+            "error_flags": [int(e64), int(e32), int(esw)],
             "fp64_fallback_particles": redo,
+            "stray_particle_substeps": {"fp64": strays.get(im.FORM_FP64), "fp32": strays.get(im.FORM_FP32)},
         }
 
     # --- end to end: one frame through the public API with host buffers

@@ -178,6 +178,7 @@ def _lib():
                 "icm_force_history": (i, [vp, vp, i]),
                 "icm_fp64_redo_count": (i, [vp, C.POINTER(C.c_ulonglong)]),
                 "icm_stray_count": (i, [vp, C.POINTER(C.c_ulonglong)]),
+                "icm_set_rebin_interval": (i, [vp, i]),
                 "icm_record_start": (i, [vp]), "icm_record_stop": (i, [vp]),
                 "icm_elapsed_ms": (i, [vp, C.POINTER(C.c_float)]),
                 "icm_stream": (vp, [vp]),
@@ -372,6 +373,10 @@ class GPU_Implementation5:
         v = C.c_ulonglong(0)
         _check(_lib().icm_fp64_redo_count(self._ctx, C.byref(v)))
         return int(v.value)
+
+    def set_rebin_interval(self, substeps: int) -> None:
+        self.initialize()
+        _check(_lib().icm_set_rebin_interval(self._ctx, substeps))
 
     def stray_count(self) -> int:
         v = C.c_ulonglong(0)

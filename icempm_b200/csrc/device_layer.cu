@@ -75,6 +75,11 @@ struct Fused {
     size_t cap_pts = 0, cap_nodes = 0, cap_tiles = 0;
     Parts64 p64{};
     Parts32 p32{};
+    // spare slot arrays for re-binning (same form), swapped with the above
+    Parts64 s64{};
+    Parts32 s32{};
+    int *spare_pid = nullptr, *slot_key = nullptr;
+    size_t spare_cap = 0;
     void *grid[3] = {nullptr, nullptr, nullptr};
     uint8_t *dirty = nullptr;  // 3 * cap_tiles
 };
@@ -87,6 +92,7 @@ struct icm_ctx {
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     int form = ICM_FORM_FP64_STEPWISE;
     int tile_variant = 1, threads = 128;
+    int rebin_interval = 200;
 
     icy_SimParams prms{};
     size_t cap_pts = 0, cap_nodes = 0, pts_pitch = 0, grid_pitch = 0;
@@ -175,8 +181,20 @@ static Consts32 make_consts32(const icy_SimParams &P)
     return k;
 }
 
+static void free_spare(icm_ctx *c)
+{
+    dfree(c->fz.s64.pos); dfree(c->fz.s64.F); dfree(c->fz.s64.Jp); dfree(c->fz.s64.meta);
+    dfree(c->fz.s64.vel); dfree(c->fz.s64.Bp); dfree(c->fz.s64.pq);
+    dfree(c->fz.s32.cell); dfree(c->fz.s32.frac); dfree(c->fz.s32.H); dfree(c->fz.s32.Jp);
+    dfree(c->fz.s32.meta); dfree(c->fz.s32.vel); dfree(c->fz.s32.Bp); dfree(c->fz.s32.pq);
+    dfree(c->fz.spare_pid);
+    dfree(c->fz.slot_key);
+    c->fz.spare_cap = 0;
+}
+
 static void free_fused(icm_ctx *c)
 {
+    free_spare(c);
     dfree(c->fz.p64.pos); dfree(c->fz.p64.F); dfree(c->fz.p64.Jp); dfree(c->fz.p64.meta);
     dfree(c->fz.p64.vel); dfree(c->fz.p64.Bp); dfree(c->fz.p64.pq);
     dfree(c->fz.p32.cell); dfree(c->fz.p32.frac); dfree(c->fz.p32.H); dfree(c->fz.p32.Jp);
@@ -258,6 +276,7 @@ static int ensure_slots(icm_ctx *c, int form, size_t nslots)
     dfree(c->fz.p32.cell); dfree(c->fz.p32.frac); dfree(c->fz.p32.H); dfree(c->fz.p32.Jp);
     dfree(c->fz.p32.meta); dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
     dfree(c->bin.pid);
+    free_spare(c);
     c->fz.form = form;
     c->fz.cap_pts = nslots;
     c->bin.cap_slots = nslots;
@@ -427,6 +446,110 @@ static int launch_variant(icm_ctx *c, int mode, int ntiles, const icy_SimParams 
     }
 }
 
+// Spare arrays of nslots slots for the current form (vel/Bp are not copied by
+// re-binning; the spare set gets them anyway so that a swap keeps every
+// array valid in size).
+static int ensure_spare(icm_ctx *c, size_t nslots)
+{
+    if (c->fz.spare_cap >= nslots) return ICM_OK;
+    free_spare(c);
+    int rc;
+    if ((rc = dalloc(&c->fz.spare_pid, nslots)) || (rc = dalloc(&c->fz.slot_key, nslots))) return rc;
+    if (c->fz.form == ICM_FORM_FP64) {
+        Parts64 &A = c->fz.s64;
+        if ((rc = dalloc(&A.pos, nslots)) || (rc = dalloc(&A.F, nslots)) || (rc = dalloc(&A.Jp, nslots)) ||
+            (rc = dalloc(&A.meta, nslots)) || (rc = dalloc(&A.vel, nslots)) || (rc = dalloc(&A.Bp, nslots)) ||
+            (rc = dalloc(&A.pq, nslots)))
+            return rc;
+    } else {
+        Parts32 &A = c->fz.s32;
+        if ((rc = dalloc(&A.cell, nslots)) || (rc = dalloc(&A.frac, nslots)) || (rc = dalloc(&A.H, nslots)) ||
+            (rc = dalloc(&A.Jp, nslots)) || (rc = dalloc(&A.meta, nslots)) || (rc = dalloc(&A.vel, nslots)) ||
+            (rc = dalloc(&A.Bp, nslots)) || (rc = dalloc(&A.pq, nslots)))
+            return rc;
+    }
+    c->fz.spare_cap = nslots;
+    return ICM_OK;
+}
+
+// Re-bins the internal (slot-ordered) particle arrays by their current base
+// nodes. Only valid between steady-state launches of a run.
+static int rebin_internal(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
+{
+    TileGeom g;
+    int ntiles;
+    geometry(P, c->internal_variant, g, ntiles);
+    const size_t ncells = (size_t)ntiles * g.TX * g.TY;
+    const int ngroups = (int)(ncells / 32);
+    const int ns_old = c->nslots, n = P.nPts;
+    cudaStream_t s = c->stream;
+    int rc = ensure_spare(c, (size_t)std::max(ns_old, 1));
+    if (rc) return rc;
+    ICM_CUDA(cudaMemsetAsync(c->bin.count, 0, sizeof(int) * (ncells + 1), s));
+    const Consts32 K32 = make_consts32(P);
+    const Pol64::Consts K64{0};
+    if (ns_old > 0) {
+        if (c->fz.form == ICM_FORM_FP64)
+            k_rebin_keys<Pol64><<<(ns_old + 255) / 256, 256, 0, s>>>(P, K64, g, ns_old, c->bin.pid, c->fz.p64,
+                                                                       c->fz.slot_key, c->bin.count);
+        else
+            k_rebin_keys<Pol32><<<(ns_old + 255) / 256, 256, 0, s>>>(P, K32, g, ns_old, c->bin.pid, c->fz.p32,
+                                                                       c->fz.slot_key, c->bin.count);
+        ICM_LAUNCHED("k_rebin_keys");
+    }
+    if ((rc = scan_ints(c, c->bin.count, (int)ncells, c->bin.chunk, c->bin.cell_start))) return rc;
+    ICM_CUDA(cudaMemcpyAsync(c->bin.cursor, c->bin.cell_start, sizeof(int) * ncells, cudaMemcpyDeviceToDevice, s));
+    if (ns_old > 0) {
+        k_rebin_scatter<<<(ns_old + 255) / 256, 256, 0, s>>>(ns_old, c->bin.pid, c->fz.slot_key, c->bin.cursor,
+                                                            c->bin.perm);
+        ICM_LAUNCHED("k_rebin_scatter");
+    }
+    k_rebin_order<<<(int)((ncells + 255) / 256), 256, 0, s>>>((int)ncells, c->bin.cell_start, c->bin.perm, c->bin.pid);
+    ICM_LAUNCHED("k_rebin_order");
+    k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start);
+    ICM_LAUNCHED("k_tile_starts");
+    k_group_slots<<<(ngroups + 255) / 256, 256, 0, s>>>(ngroups, c->bin.cell_start, c->bin.group_slots);
+    ICM_LAUNCHED("k_group_slots");
+    if ((rc = scan_ints(c, c->bin.group_slots, ngroups, c->bin.gchunk, c->bin.group_base))) return rc;
+    int ns_new = 0;
+    ICM_CUDA(cudaMemcpyAsync(&ns_new, c->bin.group_base + ngroups, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICM_CUDA(cudaStreamSynchronize(s));
+    if ((size_t)ns_new > c->fz.spare_cap) {
+        // the spare set must hold the new layout; grow it (contents of the
+        // current set are untouched)
+        free_spare(c);
+        if ((rc = ensure_spare(c, (size_t)ns_new))) return rc;
+        // slot keys were lost with the old spare set: recompute them
+        ICM_CUDA(cudaMemsetAsync(c->bin.count, 0, sizeof(int) * (ncells + 1), s));
+        if (c->fz.form == ICM_FORM_FP64)
+            k_rebin_keys<Pol64><<<(ns_old + 255) / 256, 256, 0, s>>>(P, K64, g, ns_old, c->bin.pid, c->fz.p64,
+                                                                       c->fz.slot_key, c->bin.count);
+        else
+            k_rebin_keys<Pol32><<<(ns_old + 255) / 256, 256, 0, s>>>(P, K32, g, ns_old, c->bin.pid, c->fz.p32,
+                                                                       c->fz.slot_key, c->bin.count);
+        ICM_LAUNCHED("k_rebin_keys");
+    }
+    ICM_CUDA(cudaMemsetAsync(c->fz.spare_pid, 0xff, sizeof(int) * (size_t)std::max(ns_new, 1), s));
+    if (n > 0) {
+        if (c->fz.form == ICM_FORM_FP64)
+            k_rebin_gather<Parts64><<<(n + 255) / 256, 256, 0, s>>>(n, c->bin.perm, c->fz.slot_key, c->bin.cell_start,
+                                                                    c->bin.group_base, c->bin.pid, c->fz.spare_pid,
+                                                                    c->fz.p64, c->fz.s64, keep_pq ? 1 : 0);
+        else
+            k_rebin_gather<Parts32><<<(n + 255) / 256, 256, 0, s>>>(n, c->bin.perm, c->fz.slot_key, c->bin.cell_start,
+                                                                    c->bin.group_base, c->bin.pid, c->fz.spare_pid,
+                                                                    c->fz.p32, c->fz.s32, keep_pq ? 1 : 0);
+        ICM_LAUNCHED("k_rebin_gather");
+    }
+    std::swap(c->fz.p64, c->fz.s64);
+    std::swap(c->fz.p32, c->fz.s32);
+    std::swap(c->bin.pid, c->fz.spare_pid);
+    std::swap(c->fz.cap_pts, c->fz.spare_cap);
+    c->bin.cap_slots = c->fz.cap_pts;
+    c->nslots = ns_new;
+    return ICM_OK;
+}
+
 static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
 {
     icy_SimParams P = kernel_params(c, p);
@@ -505,6 +628,10 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
         R.record_pq = ((p->SimulationStep + k) % p->UpdateEveryNthStep == 0) ? 1 : 0;
         any_pq |= R.record_pq != 0;
         if ((rc = launch(k < n ? kModeFull : kModeFinal))) return rc;
+        if (k < n && c->rebin_interval > 0 && k % c->rebin_interval == 0) {
+            if ((rc = rebin_internal(c, P, c->internal_pq || any_pq))) return rc;
+            R.group_base = c->bin.group_base;
+        }
     }
     p->SimulationStep += n;
     p->SimulationTime = t;
@@ -622,6 +749,14 @@ extern "C" int icm_set_tile(icm_ctx *c, int variant, int threads)
     }
     c->tile_variant = variant;
     c->threads = threads;
+    return ICM_OK;
+}
+
+extern "C" int icm_set_rebin_interval(icm_ctx *c, int substeps)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    if (substeps < 0) return icm::fail(ICM_ERR_ARG, "re-binning interval must be >= 0");
+    c->rebin_interval = substeps;
     return ICM_OK;
 }
 

@@ -1086,3 +1086,93 @@ __global__ void k_unpack32(const icy_SimParams P, int nslots, const int *pid, co
 }
 
 }  // namespace icm
+
+// ------------------------------------------------------------- re-binning
+//
+// Particles drift out of the cell they were binned to; such "strays" take
+// the per-particle scatter path. Between two steady-state launches the
+// internal arrays are re-binned: keys from the current positions, a
+// counting sort (deterministic inside a cell: particle order), new ELL slots
+// and a gather into the spare arrays. Velocity and Bp are not part of the
+// state between launches (the next G2P rebuilds them from the grid), and
+// the scatter buffer of the next substep is already filled, so nothing else
+// moves.
+
+namespace icm {
+
+__device__ __forceinline__ int key_of_base(const icy_SimParams &P, const TileGeom &g, int bx, int by)
+{
+    bx = min(max(bx, 0), P.GridX - 1);
+    by = min(max(by, 0), P.GridY - 1);
+    int tx = bx / g.TX, ty = by / g.TY;
+    return ((ty * g.ntx + tx) * g.TY + (by - ty * g.TY)) * g.TX + (bx - tx * g.TX);
+}
+
+template <class Pol>
+__global__ void k_rebin_keys(const icy_SimParams P, const typename Pol::Consts K, const TileGeom g, int nslots,
+                             const int *pid, const typename Pol::Parts A, int *slot_key, int *count)
+{
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslots || pid[slot] < 0) return;
+    typename Pol::St s = Pol::load(A, slot);
+    typename Pol::Sten st = Pol::stencil(P, K, s);
+    int k = key_of_base(P, g, st.bx, st.by);
+    slot_key[slot] = k;
+    atomicAdd(&count[k], 1);
+}
+
+__global__ void k_rebin_scatter(int nslots, const int *pid, const int *slot_key, int *cursor, int *order)
+{
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslots || pid[slot] < 0) return;
+    int pos = atomicAdd(&cursor[slot_key[slot]], 1);
+    order[pos] = slot;
+}
+
+// Insertion sort of each cell's slots by particle id (the atomic scatter
+// order is not deterministic).
+__global__ void k_rebin_order(int ncells, const int *start, int *order, const int *pid)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    int a = start[c], b = start[c + 1];
+    for (int i = a + 1; i < b; i++) {
+        int v = order[i], pv = pid[v], j = i - 1;
+        while (j >= a && pid[order[j]] > pv) { order[j + 1] = order[j]; j--; }
+        order[j + 1] = v;
+    }
+}
+
+__device__ __forceinline__ void copy_slot(const Parts32 &S, int from, const Parts32 &D, int to, bool pq)
+{
+    D.cell[to] = S.cell[from];
+    D.frac[to] = S.frac[from];
+    D.H[to] = S.H[from];
+    D.Jp[to] = S.Jp[from];
+    D.meta[to] = S.meta[from];
+    if (pq) D.pq[to] = S.pq[from];
+}
+__device__ __forceinline__ void copy_slot(const Parts64 &S, int from, const Parts64 &D, int to, bool pq)
+{
+    D.pos[to] = S.pos[from];
+    D.F[to] = S.F[from];
+    D.Jp[to] = S.Jp[from];
+    D.meta[to] = S.meta[from];
+    if (pq) D.pq[to] = S.pq[from];
+}
+
+template <class Parts>
+__global__ void k_rebin_gather(int n, const int *order, const int *slot_key, const int *cell_start,
+                               const int *group_base, const int *pid_old, int *pid_new, const Parts S, const Parts D,
+                               int pq)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    int old = order[q];
+    int k = slot_key[old];
+    int ns = group_base[k >> 5] + 32 * (q - cell_start[k]) + (k & 31);
+    copy_slot(S, old, D, ns, pq != 0);
+    pid_new[ns] = pid_old[old];
+}
+
+}  // namespace icm

@@ -106,6 +106,11 @@ int icm_get_form(icm_ctx *ctx);
  * 16x16 nodes, 128 threads). */
 int icm_set_tile(icm_ctx *ctx, int tile_variant, int threads);
 int icm_get_tile(icm_ctx *ctx, int *tile_variant, int *threads);
+/* Fused forms: re-bin the particles by their current grid cell every
+ * `substeps` substeps inside icm_run_substeps (0: only when a run starts;
+ * default 200). Particles that left their binned cell take a slower scatter
+ * path until then. */
+int icm_set_rebin_interval(icm_ctx *ctx, int substeps);
 /* GPU_Implementation5::cuda_allocate_arrays (gpu_implementation5.cu:481-513):
  * device particle SoA, grid and force bins. Writes the device pointers and
  * pitches into *p and resets the error code. */
