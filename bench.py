@@ -17,6 +17,7 @@ the substep has no cross-GPU exchange), scaling "weak".
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -32,6 +33,7 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-updates/s at 1M pts: FP32/learned vs plain FP64, 1 B200, ≤1% force err"
 UNIT = "particle-updates/s"
 L2_FLUSH_BYTES = 256 << 20
+SENS_NOISE = 3e-8  # std of the initial Fe perturbation of the FP64 sensitivity run
 
 
 def parse():
@@ -352,6 +354,19 @@ def main():
         h64, s64, e64 = res[im.FORM_FP64]
         h32, s32, e32 = res[im.FORM_FP32]
         hsw, ssw, esw = res[im.FORM_FP64_STEPWISE]
+        # sensitivity of the FP64 form itself: the same run from an initial
+        # Fe perturbed by seeded N(0, 3e-8) noise
+        mm = make(im.FORM_FP64, tile64, threads64)
+        S = mm.gpu.soa()
+        S.Fe[:] += SENS_NOISE * np.random.default_rng(1).standard_normal(S.Fe.shape)
+        mm.gpu.transfer_ponts_to_device()
+        mm.gpu.run_substeps(mm.prms, nsub)
+        hps = mm.gpu.force_history(nsub)
+        mm.gpu.cuda_transfer_from_device()
+        mm.gpu.synchronize()
+        sps = mm.gpu.tmp_transfer_buffer.copy()
+        mm.gpu.close()
+        fps = np.hypot(hps[:, 0], hps[:, 1])
         f64 = np.hypot(h64[:, 0], h64[:, 1])
         f32 = np.hypot(h32[:, 0], h32[:, 1])
         fsw = np.hypot(hsw[:, 0], hsw[:, 1])
@@ -379,6 +394,14 @@ def main():
                 "max_pos_err_h": float(np.abs(ssw[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n] - x64).max() /
                                        p0.cellsize),
             },
+            "fp64_perturbed_vs_fp64": {
+                "initial_fe_noise": SENS_NOISE,
+                "peak_force_rel_err": float(abs(fps.max() - f64.max()) / max(f64.max(), 1e-30)),
+                "max_pos_err_h": float(np.abs(sps[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n] - x64).max() /
+                                       p0.cellsize),
+                "p99_pos_err_h": float(np.percentile(np.abs(sps[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n] -
+                                                            x64).max(axis=0), 99) / p0.cellsize),
+            },
             "error_flags": [int(e64), int(e32), int(esw)],
             "fp64_fallback_particles": redo,
             "stray_particle_substeps": {"fp64": strays.get(im.FORM_FP64), "fp32": strays.get(im.FORM_FP32)},
@@ -393,9 +416,14 @@ def main():
         host = g.tmp_transfer_buffer.copy()
         bytes_soa = 8 * int(mm.prms.nPtsPitch) * 16
         d2h = bytes_soa + 8 * 2 * mm.prms.n_indenter_subdivisions + 4
+        prms0 = type(mm.prms)()
+        ctypes.memmove(ctypes.byref(prms0), ctypes.byref(mm.prms), ctypes.sizeof(prms0))
         times = []
         for k in range(1 + 2):
+            # every frame starts from the same state: particles and SimParams
+            # (time, step, indenter position)
             g.tmp_transfer_buffer[:] = host
+            ctypes.memmove(ctypes.byref(mm.prms), ctypes.byref(prms0), ctypes.sizeof(prms0))
             barrier()
             g.synchronize()
             g.record_start()
@@ -431,7 +459,9 @@ def main():
                        "substeps_per_step": args.substeps, "tile": im.TILE_VARIANTS[tile], "threads": args.threads,
                        "tile_choice": tune_note, "active_nodes": na,
                        "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
-            "gpu_launches": args.steps * (args.substeps + 1),
+            # per step: P2G prologue, substeps-1 full launches, the final
+            # launch, and the tile-order sort
+            "gpu_launches": args.steps * (args.substeps + 2),
             "roofline": roof,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,

@@ -82,6 +82,10 @@ struct Fused {
     size_t spare_cap = 0;
     void *grid[3] = {nullptr, nullptr, nullptr};
     uint8_t *dirty = nullptr;  // 3 * cap_tiles
+    // tile scheduling: measured cost and launch order per tile
+    unsigned *cost = nullptr;
+    int *order = nullptr;
+    int cost_variant = -1, cost_ntiles = -1;  // what the costs were measured on
 };
 
 }  // namespace
@@ -161,15 +165,6 @@ static Consts32 make_consts32(const icy_SimParams &P)
     k.stress_c = (float)((P.InitialTimeStep * P.ParticleVolume) * P.Dp_inv);
     k.mu = (float)P.mu;
     k.kappa = (float)P.kappa;
-    k.tan_phi = (float)P.DP_tan_phi;
-    k.p_thr = (float)P.DP_threshold_p;
-    k.pmax_dp = (float)P.IceCompressiveStrength;
-    k.qmax_dp = (float)P.IceShearStrength;
-    double Je_new = std::sqrt(1.0 + 2.0 * P.DP_threshold_p / P.kappa);
-    k.tension_Je_new = (float)Je_new;
-    double a = 2.0 * P.DP_threshold_p / P.kappa;
-    double jm1 = a / (std::sqrt(1.0 + a) + 1.0);
-    k.tension_delta = (float)(jm1 / (std::sqrt(Je_new) + 1.0));
     k.gv = (float)P.GrainVariability;
     k.ics = (float)(P.IceCompressiveStrength * 1e-6);
     k.its = (float)(P.IceTensileStrength * 1e-6);
@@ -177,7 +172,6 @@ static Consts32 make_consts32(const icy_SimParams &P)
     k.four_h_inv = (float)(4.0 * P.cellsize_inv);
     k.dt_g = (float)(P.InitialTimeStep * P.Gravity);
     k.vmax = (float)(0.5 * P.cellsize / P.InitialTimeStep);
-    k.half_inv_mu = (float)(1.0 / (2.0 * P.mu));
     return k;
 }
 
@@ -201,6 +195,7 @@ static void free_fused(icm_ctx *c)
     dfree(c->fz.p32.meta); dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
     for (int b = 0; b < 3; b++) { if (c->fz.grid[b]) cudaFree(c->fz.grid[b]); c->fz.grid[b] = nullptr; }
     dfree(c->fz.dirty);
+    dfree(c->fz.cost); dfree(c->fz.order);
     c->fz = Fused{};
 }
 
@@ -227,6 +222,8 @@ static int ensure_grids(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t
     if (c->fz.form != form || c->fz.cap_nodes < nnodes || c->fz.cap_tiles < ntiles) {
         for (int b = 0; b < 3; b++) { if (c->fz.grid[b]) cudaFree(c->fz.grid[b]); c->fz.grid[b] = nullptr; }
         dfree(c->fz.dirty);
+        dfree(c->fz.cost); dfree(c->fz.order);
+        c->fz.cost_variant = -1;
         c->fz.cap_nodes = nnodes;
         c->fz.cap_tiles = ntiles;
         int rc = ICM_OK;
@@ -241,7 +238,9 @@ static int ensure_grids(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t
                 c->fz.grid[b] = g;
             }
         }
-        if ((rc = dalloc(&c->fz.dirty, 3 * ntiles))) return rc;
+        if ((rc = dalloc(&c->fz.dirty, 3 * ntiles)) || (rc = dalloc(&c->fz.cost, ntiles)) ||
+            (rc = dalloc(&c->fz.order, ntiles)))
+            return rc;
     }
     if (c->bin.cap_pts < npts || c->bin.cap_cells < ncells || c->bin.cap_tiles < ntiles) {
         int *pid = c->bin.pid;  // slot-sized, managed by ensure_slots
@@ -550,6 +549,32 @@ static int rebin_internal(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
     return ICM_OK;
 }
 
+// Tile order for the next launches: by the costs measured on this tile
+// geometry, or the identity (null) while there are none.
+static int tile_order(icm_ctx *c, int ntiles, const int *&order)
+{
+    order = nullptr;
+    if (c->fz.cost_variant != c->tile_variant || c->fz.cost_ntiles != ntiles) {
+        ICM_CUDA(cudaMemsetAsync(c->fz.cost, 0, sizeof(unsigned) * (size_t)ntiles, c->stream));
+        c->fz.cost_variant = c->tile_variant;
+        c->fz.cost_ntiles = ntiles;
+        return ICM_OK;
+    }
+    if (ntiles > kMaxOrderTiles) return ICM_OK;
+    int m = 1;
+    while (m < ntiles) m <<= 1;
+    static bool opted = false;
+    if (!opted) {
+        ICM_CUDA(cudaFuncSetAttribute(k_tile_order, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(unsigned long long) * kMaxOrderTiles)));
+        opted = true;
+    }
+    k_tile_order<<<1, kOrderThreads, sizeof(unsigned long long) * m, c->stream>>>(ntiles, c->fz.cost, c->fz.order);
+    ICM_LAUNCHED("k_tile_order");
+    order = c->fz.order;
+    return ICM_OK;
+}
+
 static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
 {
     icy_SimParams P = kernel_params(c, p);
@@ -586,6 +611,8 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     R.group_base = c->bin.group_base;
     R.strays = c->d_strays;
     R.ind_y = p->indenter_y;
+    R.cost = c->fz.cost;
+    if ((rc = tile_order(c, ntiles, R.order))) return rc;
 
     const Consts32 K32 = make_consts32(P);
     const Pol64::Consts K64{0};
@@ -631,6 +658,7 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
         if (k < n && c->rebin_interval > 0 && k % c->rebin_interval == 0) {
             if ((rc = rebin_internal(c, P, c->internal_pq || any_pq))) return rc;
             R.group_base = c->bin.group_base;
+            if ((rc = tile_order(c, ntiles, R.order))) return rc;
         }
     }
     p->SimulationStep += n;

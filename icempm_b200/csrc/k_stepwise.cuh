@@ -129,7 +129,7 @@ __global__ void k_g2p_ref64(const icy_SimParams P, int recordPQ)
     M2d Fn = {M00 * F.a00 + M01 * F.a10, M00 * F.a01 + M01 * F.a11, M10 * F.a00 + M11 * F.a10,
               M10 * F.a01 + M11 * F.a11};
     double p_tr, q_tr;
-    constitutive64(P, Fn, Jp, crushed, grain, p_tr, q_tr);
+    constitutive64(P, Fn, Jp, crushed, grain_res(grain), p_tr, q_tr);
 
     pts_row(P, ICM_IDX_JP_INV)[pt] = Jp;
     pts_row(P, ICM_IDX_POSX)[pt] = x;

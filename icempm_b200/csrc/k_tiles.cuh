@@ -85,6 +85,10 @@ struct TileRun {
     const int *cell_start;          // binning: cell key k holds cell_start[k+1] - cell_start[k] particles
     const int *group_base;          // first slot of each group of 32 consecutive cell keys
     unsigned long long *strays;     // particles that left their binned cell (count)
+    // tile scheduling: CTA i runs tile order[i] (tile i when null); a full
+    // substep launch writes tile t's clock cycles to cost[t]
+    const int *order;
+    unsigned *cost;
 };
 
 struct Parts64 { double2 *pos; double4 *F; double *Jp; uint32_t *meta; double2 *vel; double4 *Bp; double2 *pq; };
@@ -102,6 +106,8 @@ template <class T> struct Tau { T t00, t01, t10, t11; };
 // FP64 reference form: absolute positions, Fe, Jp_inv in double; meta is
 // the grain id (bits 0-15) and the crushed flag (bits 16-23).
 struct Pol64 {
+    // Bp from raw node velocities, operation order of the reference
+    static constexpr bool kRelativeGradient = false;
     using real = double;
     using V2 = double2;
     using Node = Node64;
@@ -182,7 +188,7 @@ struct Pol64 {
         M2d F = s.F;
         s.F = {M00 * F.a00 + M01 * F.a10, M00 * F.a01 + M01 * F.a11, M10 * F.a00 + M11 * F.a10, M10 * F.a01 + M11 * F.a11};
         uint8_t cr = (uint8_t)(s.meta >> 16);
-        constitutive64(P, s.F, s.Jp, cr, (int)(int16_t)(s.meta & 0xffffu), p_tr, q_tr);
+        constitutive64(P, s.F, s.Jp, cr, grain_res((int)(int16_t)(s.meta & 0xffffu)), p_tr, q_tr);
         s.meta = (s.meta & 0xffffu) | ((uint32_t)cr << 16);
         redo = 0;
         return stress(P, K, s);
@@ -206,6 +212,12 @@ struct Pol64 {
 // FP32 strain form: position = int16 cell + FP32 fraction, H = Fe - I; meta
 // holds the grain's residues and the crushed flag (grain_meta32).
 struct Pol32 {
+    // Bp = 4/h sum W (v_i - v_c) dpos^T with v_c the stencil's centre node:
+    // equal to the reference's sum since sum W dpos = 0, but free of the
+    // cancellation of a large common velocity (whose FP32 residual would
+    // repeat substep after substep for a slowly moving particle and add up
+    // in Fe over thousands of substeps)
+    static constexpr bool kRelativeGradient = true;
     using real = float;
     using V2 = float2;
     using Node = float4;
@@ -355,7 +367,7 @@ struct Pol32 {
         s.H.a11 = H.a11 + (c11 + (c10 * H.a01 + c11 * H.a11));
         redo = 0;
         Tau32 t;
-        if (constitutive32(k, T, s.H, s.Jp, s.meta, p_tr, q_tr, t) == kC32_NEEDS_FP64) {
+        if (constitutive32(k, T, s.H, s.meta, p_tr, q_tr, t) == kC32_NEEDS_FP64) {
             constitutive32_via64(P, s.H, s.Jp, s.meta, p_tr, q_tr);
             redo = 1;
             return stress(P, k, s);
@@ -444,10 +456,11 @@ __host__ __device__ constexpr size_t tile_dyn_bytes(int RN, int nwarps)
     return tile_region_bytes<Pol, MODE>(RN, nwarps) + (size_t)nwarps * 2 * sizeof(typename Pol::Stage);
 }
 
+// One substep of one tile (the body of k_tile_substep). Every return is
+// uniform over the CTA.
 template <class Pol, int TX, int TY, int MODE>
-__global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ icy_SimParams P,
-                                                      const __grid_constant__ typename Pol::Consts K,
-                                                      const typename Pol::Parts A, const TileRun R)
+__device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename Pol::Consts &K,
+                                          const typename Pol::Parts &A, const TileRun &R, const int t)
 {
     using real = typename Pol::real;
     using V2 = typename Pol::V2;
@@ -465,7 +478,6 @@ __global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ ic
     __shared__ int s_wcnt[kMaxWarps][kMaxGroupsPerWarp][32];
     __shared__ int s_wrounds[kMaxWarps][kMaxGroupsPerWarp], s_wgbase[kMaxWarps][kMaxGroupsPerWarp];
 
-    const int t = blockIdx.x;
     const int tx = t % R.ntx, ty = t / R.ntx;
     const int x0 = tx * TX, y0 = ty * TY;
     const int rx0 = x0 - 1, ry0 = y0 - 1;
@@ -667,32 +679,45 @@ __global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ ic
                 const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 && st.by >= 0 &&
                                     st.bx + 2 < GX && st.by + 2 < GY;
                 real a[3][2], b[3][2];
+                real vc0 = 0, vc1 = 0;  // reference velocity of the relative form
                 if (inside) {
                     const int q0 = ly * RX + lx;
+                    if (Pol::kRelativeGradient) {
+                        const V2 c = s_v[q0 + RX + 1];
+                        vc0 = c.x;
+                        vc1 = c.y;
+                    }
 #pragma unroll
                     for (int i = 0; i < 3; i++) {
                         a[i][0] = 0; a[i][1] = 0; b[i][0] = 0; b[i][1] = 0;
 #pragma unroll
                         for (int j = 0; j < 3; j++) {
                             const V2 n = s_v[q0 + j * RX + i];
+                            const real n0 = n.x - vc0, n1 = n.y - vc1;
                             const real wyd = st.wy[j] * ((real)j - st.fy);
-                            a[i][0] += st.wy[j] * n.x;
-                            a[i][1] += st.wy[j] * n.y;
-                            b[i][0] += wyd * n.x;
-                            b[i][1] += wyd * n.y;
+                            a[i][0] += st.wy[j] * n0;
+                            a[i][1] += st.wy[j] * n1;
+                            b[i][0] += wyd * n0;
+                            b[i][1] += wyd * n1;
                         }
                     }
                 } else {
+                    if (Pol::kRelativeGradient) {
+                        Pair<real> c = far_node_velocity<Pol>(P, K, gA, st.bx + 1, st.by + 1, R.ind_x, R.ind_y);
+                        vc0 = c.a;
+                        vc1 = c.b;
+                    }
 #pragma unroll 1
                     for (int i = 0; i < 3; i++) {
                         a[i][0] = 0; a[i][1] = 0; b[i][0] = 0; b[i][1] = 0;
                         for (int j = 0; j < 3; j++) {
                             Pair<real> n = far_node_velocity<Pol>(P, K, gA, st.bx + i, st.by + j, R.ind_x, R.ind_y);
+                            const real n0 = n.a - vc0, n1 = n.b - vc1;
                             const real wyd = st.wy[j] * ((real)j - st.fy);
-                            a[i][0] += st.wy[j] * n.a;
-                            a[i][1] += st.wy[j] * n.b;
-                            b[i][0] += wyd * n.a;
-                            b[i][1] += wyd * n.b;
+                            a[i][0] += st.wy[j] * n0;
+                            a[i][1] += st.wy[j] * n1;
+                            b[i][0] += wyd * n0;
+                            b[i][1] += wyd * n1;
                         }
                     }
                 }
@@ -707,6 +732,8 @@ __global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ ic
                     B[3] += st.wx[i] * b[i][1];
                 }
                 B[0] *= fhi; B[1] *= fhi; B[2] *= fhi; B[3] *= fhi;
+                v0 += vc0;  // sum W = 1
+                v1 += vc1;
                 real p_tr, q_tr;
                 int redo;
                 tau = Pol::advance(P, K, s_tab, s, v0, v1, B, p_tr, q_tr, redo);
@@ -820,6 +847,60 @@ __global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ ic
         int ntx2 = tx + tid % 3 - 1, nty2 = ty + tid / 3 - 1;
         if (ntx2 >= 0 && nty2 >= 0 && ntx2 < R.ntx && nty2 < R.nty) R.dirty[R.bufB][nty2 * R.ntx + ntx2] = 1;
     }
+}
+
+// One launch = one substep over all tiles, one CTA per tile. Tile costs are
+// uneven (indenter contact, crushed particles redone in FP64, occupancy), so
+// CTA i takes tile order[i] -- the tiles sorted by the cost measured in
+// earlier launches, heaviest first, which the hardware dispatches first --
+// instead of letting late heavy tiles form the tail of the launch.
+template <class Pol, int TX, int TY, int MODE>
+__global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ icy_SimParams P,
+                                                      const __grid_constant__ typename Pol::Consts K,
+                                                      const typename Pol::Parts A, const __grid_constant__ TileRun R)
+{
+    __shared__ long long s_clock;
+    const int t = R.order ? R.order[blockIdx.x] : blockIdx.x;
+    if (MODE == kModeFull && threadIdx.x == 0) s_clock = clock64();
+    tile_body<Pol, TX, TY, MODE>(P, K, A, R, t);
+    if (MODE == kModeFull && R.cost) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const long long dc = clock64() - s_clock;
+            R.cost[t] = (unsigned)(dc < 0 ? 0 : (dc > 0xffffffffll ? 0xffffffffll : dc));
+        }
+    }
+}
+
+// Tile order by descending cost (ties by tile index): a bitonic sort of
+// (cost << 32 | ~tile) keys in shared memory, one CTA, n <= kMaxOrderTiles.
+constexpr int kMaxOrderTiles = 8192;
+constexpr int kOrderThreads = 1024;
+
+__global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsigned *cost, int *order)
+{
+    extern __shared__ unsigned long long s_key[];
+    int m = 1;
+    while (m < n) m <<= 1;
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+        s_key[i] = (i < n) ? (((unsigned long long)cost[i] << 32) | (0xffffffffu - (unsigned)i)) : 0ull;
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const unsigned long long a = s_key[i], b = s_key[l];
+                    const bool desc = (i & k) == 0;
+                    if (desc ? (a < b) : (a > b)) {
+                        s_key[i] = b;
+                        s_key[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) order[i] = (int)(0xffffffffu - (unsigned)(s_key[i] & 0xffffffffu));
 }
 
 // ------------------------------------------------ binning, pack and unpack

@@ -15,17 +15,16 @@
 //   p = -kappa/2 (J^2 - 1) = -s2/2,
 //   q = sqrt(2) |mu/J dev(sigma^2)| = (mu/J)(sigma0^2 - sigma1^2)
 //     = 2 s1 sqrt(hd^2 + b01^2).
-// Only a crushed particle needs U and V (the Drucker-Prager map rebuilds Fe
-// from them, gpu_implementation5.cu:48-94); its SVD follows the reference's
-// route (polar decomposition, then a symmetric eigen-solve,
-// helper_math.cuh:27-46,81-140) in strain form: F = R S, S = I + E with E
-// from H and cos(theta) - 1 = -b^2/(d(a+d)); sigma_i = 1 + e_i. The
-// projected stretches enter as delta_i = sigma_new_i - 1 =
-// (B_i - 1)/(sqrt(B_i) + 1) and H_new = R V diag(delta) V^T + (R - I).
-// Where this is ill-conditioned -- det F small or negative, a large rotation
-// (tr F <= 0.5), large strain, or nearly equal singular values of a crushed
-// particle -- the caller redoes the particle in FP64 with the reference form
-// (mpm_math64.cuh).
+// An intact particle whose (p, q) is clearly inside its failure surface is
+// done here in FP32. Everything else -- the crush decision at the surface,
+// every crushed particle (SVD + Drucker-Prager map, gpu_implementation5.cu:
+// 48-94, helper_math.cuh:27-140) and ill-conditioned states (det F small or
+// negative) -- is redone in FP64 with the reference form (mpm_math64.cuh).
+// Crushed particles are a fraction of a percent of a block and sit together
+// near the indenter, so this costs no measurable time; it is done for all of
+// them, not only for nearly equal singular values, because the indentation's
+// crushing outcome is sensitive to strain perturbations of a few 1e-8 and an
+// FP32 return map moved the peak indenter force of a 10k-substep run by ~4%.
 #pragma once
 #include <cstdint>
 #include "mpm_math64.cuh"
@@ -37,11 +36,10 @@ struct M2f { float a00, a01, a10, a11; };
 // Per-run FP32 constants, derived on the host in double.
 struct Consts32 {
     float h, h_inv, dt, dt_h_inv, mass, stress_c;  // stress_c = dt*Vp*Dinv
-    float mu, kappa, tan_phi, p_thr, pmax_dp, qmax_dp;
-    float tension_Je_new, tension_delta;            // sqrt(1 + 2 p_thr/kappa), sqrt(Je_new) - 1
+    float mu, kappa;
     float gv, ics, its, iss;                        // grain variability, strengths in MPa
     float four_h_inv;
-    float dt_g, vmax, half_inv_mu;                  // dt*gravity, 0.5 h/dt, 1/(2 mu)
+    float dt_g, vmax;                               // dt*gravity, 0.5 h/dt
 };
 
 // Grain strengths in MPa by residue (gpu_implementation5.cu:97-105): the
@@ -68,17 +66,10 @@ __host__ __device__ __forceinline__ uint32_t grain_meta32(int grain, int crushed
 }
 __device__ __forceinline__ int meta32_crushed(uint32_t m) { return (int)(m >> 24); }
 
-// A grain id with the same residues (for the FP64 redo, which evaluates
-// GetParametersForGrain): ids with equal grain % 21, (grain + 3) % 30 and
-// (grain + 4) % 11 have equal parameters; the residues repeat with period
-// 2310, searched only on that rare path.
-__device__ __forceinline__ int meta32_grain(uint32_t m)
+// The reference's grain remainders (grain_res) of a meta word.
+__device__ __forceinline__ GrainRes meta32_res(uint32_t m)
 {
-    int r1 = (int)(m & 63u) - 20, r2 = (int)((m >> 6) & 63u) - 29, r3 = (int)((m >> 12) & 31u) - 10;
-    int base = (r1 < 0 || r2 < 0 || r3 < 0) ? -2309 : 0;
-    for (int g = base; g < base + 2310; g++)
-        if (g % 21 == r1 && (g + 3) % 30 == r2 && (g + 4) % 11 == r3) return g;
-    return 0;
+    return {(int)(m & 63u) - 20, (int)((m >> 6) & 63u) - 29, (int)((m >> 12) & 31u) - 10};
 }
 
 // Stress and (p, q) of one H.
@@ -104,58 +95,6 @@ __device__ __forceinline__ Tau32 tau32(const Inv32 &v) { return {v.s1 * v.hd + v
 
 __device__ __forceinline__ float approx_sqrt(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
 
-struct Svd32 {
-    float c, s;    // R = [[c, -s], [s, c]]
-    float cm1;     // c - 1, computed without cancellation
-    float vc, vs;  // V = [[vc, -vs], [vs, vc]]: columns are the eigenvectors of S
-    float e0, e1;  // sigma_i - 1, e0 >= e1
-    float w;       // (e0 - e1)/2
-    float a;       // tr F, the polar denominator's first component
-};
-
-__device__ __forceinline__ Svd32 svd_strain32(const M2f &H)
-{
-    Svd32 r;
-    float a = 2.0f + H.a00 + H.a11;
-    float b = H.a10 - H.a01;
-    r.a = a;
-    float d = sqrtf(a * a + b * b);
-    float inv_d = 1.0f / d;
-    r.c = a * inv_d;
-    r.s = b * inv_d;
-    r.cm1 = __fdividef(-(b * b) * inv_d, a + d);
-    float E00 = r.cm1 + r.c * H.a00 + r.s * H.a10;
-    float E11 = r.cm1 - r.s * H.a01 + r.c * H.a11;
-    float E01 = r.s + r.c * H.a01 + r.s * H.a11;
-    float E10 = -r.s - r.s * H.a00 + r.c * H.a10;
-    float y = 0.5f * (E01 + E10);
-    float mean = 0.5f * (E00 + E11);
-    float tau = 0.5f * (E00 - E11);
-    float w = sqrtf(tau * tau + y * y);
-    r.w = w;
-    r.e0 = mean + w;
-    r.e1 = mean - w;
-    // eigenvector of the larger eigenvalue, from the better-conditioned row
-    float vx, vy;
-    if (tau >= 0.0f) {
-        vx = w + tau;
-        vy = y;
-    } else {
-        vx = y;
-        vy = w - tau;
-    }
-    float n2 = vx * vx + vy * vy;
-    if (n2 > 0.0f) {
-        float inv = rsqrtf(n2);
-        r.vc = vx * inv;
-        r.vs = vy * inv;
-    } else {
-        r.vc = 1.0f;
-        r.vs = 0.0f;
-    }
-    return r;
-}
-
 // Grain-varied failure surface (gpu_implementation5.cu:97-141) in FP32,
 // rearranged without divisions and in MPa so every product stays in range:
 //   p < 0:  crushed if p < -3 MPa, or if q > q0 (p + 3 MPa)/(3 MPa) with
@@ -165,90 +104,63 @@ __device__ __forceinline__ Svd32 svd_strain32(const M2f &H)
 //           beta = -pmin/pmax and M^2 = 4 qmax^2 (1 + 2 beta)/(pmax (1 + beta))^2
 //           has the sign of q^2 (pmax - pmin)^2 + 4 qmax^2 (p - pmin)(p - pmax)
 //           (1 + 2 beta > 0 and pmax (1 + beta) = pmax - pmin).
-__device__ __forceinline__ bool outside_failure_surface32(const GrainTables32 &T, uint32_t meta, float p_pa,
-                                                          float q_pa)
+// Returns 1 (outside), 0 (inside) or -1 when the point lies within a
+// relative margin of the surface, where the FP32 decision is not trusted.
+constexpr float kSurfaceMargin = 1e-3f;
+
+__device__ __forceinline__ int failure_side32(const GrainTables32 &T, uint32_t meta, float p_pa, float q_pa)
 {
     float pmax = T.pmax[meta & 63u];
     float pmin = T.pmin[(meta >> 6) & 63u];
     float qmax = T.qmax[(meta >> 12) & 31u];
     float p = p_pa * 1e-6f, q = q_pa * 1e-6f;
     float dpm = pmax - pmin;
+    // Both branches have the same sign at p = 0; at p = -3 MPa only q ~ 0 is ambiguous.
+    if (fabsf(p + 3.0f) < 3.0f * kSurfaceMargin) return -1;
     if (p < 0.0f) {
-        if (p < -3.0f) return true;
+        if (p < -3.0f) return 1;
         float l = 3.0f * q * dpm, r2 = 4.0f * (-pmax * pmin) * qmax * qmax;
         float pp = p + 3.0f;
-        return l * l > r2 * pp * pp;
+        float a = l * l, b = r2 * pp * pp;
+        if (fabsf(a - b) <= 2.0f * kSurfaceMargin * (a + b)) return -1;
+        return a > b ? 1 : 0;
     }
-    return q * q * dpm * dpm + 4.0f * qmax * qmax * (p - pmin) * (p - pmax) > 0.0f;
+    float a = q * q * dpm * dpm, b = 4.0f * qmax * qmax * (p - pmin) * (p - pmax);
+    if (fabsf(a + b) <= kSurfaceMargin * (a + fabsf(b))) return -1;
+    return a + b > 0.0f ? 1 : 0;
 }
 
 // Result codes of constitutive32.
 enum { kC32_OK = 0, kC32_NEEDS_FP64 = 1 };
 
-// ComputePQ + failure check + DP map on H (already advected). On return
-// tau holds the Kirchhoff stress of the final H. Returns kC32_NEEDS_FP64
-// without touching the state when the FP32 form is ill-conditioned.
-__device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTables32 &T, M2f &H, float &Jp_inv,
-                                              uint32_t &meta, float &p_tr, float &q_tr, Tau32 &tau)
+// ComputePQ + failure check of an intact particle whose (p, q) lies clearly
+// inside its failure surface: the state is unchanged, tau is the Kirchhoff
+// stress of H. Returns kC32_NEEDS_FP64 (state untouched) for a crushed
+// particle, for one on or outside the surface or within kSurfaceMargin of
+// it, and for det F <= 0.25.
+__device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTables32 &T, const M2f &H, uint32_t meta,
+                                              float &p_tr, float &q_tr, Tau32 &tau)
 {
     Inv32 v = invariants32(H, k.mu, k.kappa);
-    if (!(v.J > 0.25f)) return kC32_NEEDS_FP64;
-    float rad = approx_sqrt(v.hd * v.hd + v.b01 * v.b01);
+    if (!(v.J > 0.25f) || meta32_crushed(meta)) return kC32_NEEDS_FP64;
     float p = -0.5f * v.s2;
-    float q = 2.0f * v.s1 * rad;
-    uint32_t m = meta;
-    if (meta32_crushed(m) == 0 && outside_failure_surface32(T, m, p, q)) m |= 1u << 24;
-    if (meta32_crushed(m)) {
-        Svd32 d = svd_strain32(H);
-        if (!(d.a > 0.5f) || !(d.e1 > -0.5f) || !(d.e0 < 1.0f)) return kC32_NEEDS_FP64;
-        float scale = fabsf(d.e0) + fabsf(d.e1);
-        if (d.w > 0.0f && d.w < 1e-5f * scale) return kC32_NEEDS_FP64;  // nearly equal stretches
-        float d0, d1;
-        bool change = true;
-        if (p < -k.p_thr || Jp_inv < 1.0f) {
-            d0 = d1 = k.tension_delta;
-            Jp_inv *= __fdividef(k.tension_Je_new, v.J);
-        } else {
-            float q_n_1 = (p > k.pmax_dp) ? 0.0f : fminf((p + k.p_thr) * k.tan_phi, k.qmax_dp);
-            if (q >= q_n_1) {
-                float m1 = 0.5f * (d.e0 * (2.0f + d.e0) + d.e1 * (2.0f + d.e1));  // mean(sigma^2) - 1
-                float g = (rad > 0.0f) ? q_n_1 * v.J * k.half_inv_mu : 0.0f;
-                float B0 = m1 + g, B1 = m1 - g;  // B_i - 1
-                d0 = __fdividef(B0, approx_sqrt(1.0f + B0) + 1.0f);
-                d1 = __fdividef(B1, approx_sqrt(1.0f + B1) + 1.0f);
-            } else {
-                change = false;
-            }
-        }
-        if (change) {
-            // W = V diag(d0, d1) V^T; H = R W + (R - I)
-            float cc = d.vc * d.vc, ss = d.vs * d.vs, cs = d.vc * d.vs;
-            float W00 = d0 * cc + d1 * ss;
-            float W11 = d0 * ss + d1 * cc;
-            float W01 = (d0 - d1) * cs;
-            H.a00 = d.c * W00 - d.s * W01 + d.cm1;
-            H.a01 = d.c * W01 - d.s * W11 - d.s;
-            H.a10 = d.s * W00 + d.c * W01 + d.s;
-            H.a11 = d.s * W01 + d.c * W11 + d.cm1;
-            v = invariants32(H, k.mu, k.kappa);
-        }
-    }
-    meta = m;
+    float q = 2.0f * v.s1 * approx_sqrt(v.hd * v.hd + v.b01 * v.b01);
+    if (failure_side32(T, meta, p, q) != 0) return kC32_NEEDS_FP64;
     p_tr = p;
     q_tr = q;
     tau = tau32(v);
     return kC32_OK;
 }
 
-// FP64 redo of one particle for the cases constitutive32 declines (rare; kept
-// out of line).
+// FP64 redo of one particle for the cases constitutive32 declines (kept out
+// of line).
 __device__ __noinline__ void constitutive32_via64(const icy_SimParams &P, M2f &H, float &Jp_inv, uint32_t &meta,
                                                   float &p_tr, float &q_tr)
 {
     M2d F = {1.0 + (double)H.a00, (double)H.a01, (double)H.a10, 1.0 + (double)H.a11};
     double jp = Jp_inv, p, q;
     uint8_t cr = (uint8_t)meta32_crushed(meta);
-    constitutive64(P, F, jp, cr, meta32_grain(meta), p, q);
+    constitutive64(P, F, jp, cr, meta32_res(meta), p, q);
     H = {(float)(F.a00 - 1.0), (float)F.a01, (float)F.a10, (float)(F.a11 - 1.0)};
     Jp_inv = (float)jp;
     p_tr = (float)p;

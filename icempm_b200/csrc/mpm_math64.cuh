@@ -107,11 +107,16 @@ __device__ __forceinline__ M2d usvt64(const Svd64 &d, double t0, double t1)
 
 struct Grain64 { double pmin, pmax, qmax, beta, mSq; };
 
-__device__ __forceinline__ Grain64 grain_params64(const icy_SimParams &P, int grain)
+// GetParametersForGrain (gpu_implementation5.cu:97-105) depends on the grain
+// id only through these three C remainders (negative for negative ids).
+struct GrainRes { int r21, r30, r11; };
+__host__ __device__ __forceinline__ GrainRes grain_res(int grain) { return {grain % 21, (grain + 3) % 30, (grain + 4) % 11}; }
+
+__device__ __forceinline__ Grain64 grain_params64(const icy_SimParams &P, GrainRes r)
 {
-    double var1 = 1.0 + P.GrainVariability * 0.05 * (-10 + grain % 21);
-    double var2 = 1.0 + P.GrainVariability * 0.033 * (-15 + (grain + 3) % 30);
-    double var3 = 1.0 + P.GrainVariability * 0.1 * (-10 + (grain + 4) % 11);
+    double var1 = 1.0 + P.GrainVariability * 0.05 * (-10 + r.r21);
+    double var2 = 1.0 + P.GrainVariability * 0.033 * (-15 + r.r30);
+    double var3 = 1.0 + P.GrainVariability * 0.1 * (-10 + r.r11);
     Grain64 g;
     g.pmax = P.IceCompressiveStrength * var1;
     g.pmin = -P.IceTensileStrength * var2;
@@ -121,7 +126,7 @@ __device__ __forceinline__ Grain64 grain_params64(const icy_SimParams &P, int gr
     return g;
 }
 
-__device__ __forceinline__ bool outside_failure_surface64(const icy_SimParams &P, int grain, double p, double q)
+__device__ __forceinline__ bool outside_failure_surface64(const icy_SimParams &P, GrainRes grain, double p, double q)
 {
     Grain64 g = grain_params64(P, grain);
     const double pmin2 = -3e6;
@@ -139,7 +144,7 @@ __device__ __forceinline__ bool outside_failure_surface64(const icy_SimParams &P
 // ComputePQ + failure check + Drucker-Prager map on the advected Fe.
 // Updates Fe, Jp_inv and crushed in place; returns p_tr, q_tr.
 __device__ __forceinline__ void constitutive64(const icy_SimParams &P, M2d &Fe, double &Jp_inv,
-                                               uint8_t &crushed, int grain, double &p_tr, double &q_tr)
+                                               uint8_t &crushed, GrainRes grain, double &p_tr, double &q_tr)
 {
     const double mu = P.mu, kappa = P.kappa;
     Svd64 d = svd2x2_64(Fe);
