@@ -50,6 +50,8 @@ def parse():
     a.add_argument("--no-accuracy", action="store_true")
     a.add_argument("--no-cpu", action="store_true")
     a.add_argument("--no-fp64", action="store_true")
+    a.add_argument("--form", choices=["fp32", "fp64"], default="fp32",
+                   help="fused form of the headline (fp64: for profiling the FP64 fused kernel)")
     return a.parse_args()
 
 
@@ -130,19 +132,27 @@ def traffic_summary():
 
 
 def alg_bytes(form: str, n: int, na: int, ng: int) -> float:
-    """Algorithmic bytes of one steady-state substep launch.
-    fp32 fused: particle state read 36 B (cell 4, fraction 8, H 16, Jp 4,
-      meta 4) + written 28 B (cell, fraction, H); grid 48 B per active node
-      (read 16, scatter 16, zero 16).
-    fp64 fused: read 60 B (pos 16, Fe 32, Jp 8, meta 4) + written 48 B;
-      grid 96 B per active node.
-    fp64 stepwise (reference layout, three kernels): 260 B per particle +
-      32 B per node + 72 B per active node."""
+    """Algorithmic bytes of one substep of the MLS-MPM step (the roofline's
+    numerator), per particle and per node of the reference's three-kernel
+    substep (gpu_implementation5.cu:148-379):
+    FP64: P2G read 96 + G2P read 59 + G2P write 105 = 260 B per particle;
+      grid reset 24 + mass read 8 per node, P2G write 24 + update r/w 32 +
+      G2P gather 16 per active node -> 32 Ng + 72 Na.
+    FP32 (same fields in float): 48 + 31 + 53 = 132 B per particle,
+      16 Ng + 36 Na."""
+    if form == "fp32":
+        return 132.0 * n + 16.0 * ng + 36.0 * na
+    return 260.0 * n + 32.0 * ng + 72.0 * na
+
+
+def fused_min_bytes(form: str, n: int, na: int) -> float:
+    """Bytes the fused one-launch substep must move at least (its own data
+    layout): fp32 particle state read 36 B (cell 4, fraction 8, H 16, Jp 4,
+    meta 4) + written 28 B, grid 48 B per active node (read 16, scatter 16,
+    zero 16); fp64 read 60 B + written 48 B, grid 96 B per active node."""
     if form == "fp32":
         return 64.0 * n + 48.0 * na
-    if form == "fp64":
-        return 108.0 * n + 96.0 * na
-    return 260.0 * n + 32.0 * ng + 72.0 * na
+    return 108.0 * n + 96.0 * na
 
 
 def cpu_oracle_rate(name: str, budget_s: float, max_substeps: int, threads: int):
@@ -284,17 +294,18 @@ def main():
             g.kernel_timing(False)
         return ms, kt
 
+    hform = im.FORM_FP32 if args.form == "fp32" else im.FORM_FP64
     # --- tile choice (autotuner cache, else default)
     tile = args.tile
     tune_note = "fixed"
     if tile < 0:
         from icempm_b200 import autotune
 
-        tile, threads, tune_note = autotune.choose(name, im.FORM_FP32, local)
+        tile, threads, tune_note = autotune.choose(name, hform, local)
         args.threads = threads
 
-    # --- headline: FP32 fused form
-    m = make(im.FORM_FP32, tile)
+    # --- headline: FP32 fused form (or the FP64 fused form with --form fp64)
+    m = make(hform, tile)
     clocks = Clocks(local)
     ms, (kms, klaunch) = timed(m, args.steps, args.warmup, args.substeps, ktime=True, clocks=clocks)
     total_s = max_over_ranks(sum(ms) / 1e3)
@@ -304,12 +315,16 @@ def main():
 
     hbm, peak_kind = peaks()
     kavg_s = (kms / klaunch / 1e3) if klaunch else float("nan")
-    ab = alg_bytes("fp32", n, na, ng)
+    ab = alg_bytes(args.form, n, na, ng)
+    fb = fused_min_bytes(args.form, n, na)
     achieved = ab / kavg_s / 1e9
-    tr = traffic_summary().get("fp32")
+    tr = traffic_summary().get(args.form)
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": tr, "kernel": "k_tile_substep<Pol32,...,kModeFull>", "alg_bytes_per_launch": ab,
-            "avg_launch_us": kavg_s * 1e6, "launches_timed": klaunch, "peak_kind": peak_kind}
+            "traffic": tr, "kernel": f"k_tile_substep<Pol{args.form[2:]},16x16,kModeFull>" if tile == 1 else
+            f"k_tile_substep<Pol{args.form[2:]},{im.TILE_VARIANTS[tile]},kModeFull>",
+            "alg_bytes_per_launch": ab, "avg_launch_us": kavg_s * 1e6, "launches_timed": klaunch,
+            "peak_kind": peak_kind,
+            "fused_min_bytes_per_launch": fb, "frac_of_fused_min_bytes": fb / kavg_s / 1e9 / hbm}
 
     extra = {}
     # --- FP64 forms (the plain drop-in and the fused FP64 form)
@@ -330,7 +345,12 @@ def main():
                  "threads": threads64 if form == im.FORM_FP64 else None}
             if k2n:
                 a2 = alg_bytes("fp64", n, na, ng) / (k2ms / k2n / 1e3) / 1e9
-                d["roofline"] = {"achieved": a2, "frac": a2 / hbm, "avg_launch_us": 1e3 * k2ms / k2n}
+                d["roofline"] = {"achieved": a2, "frac": a2 / hbm, "avg_launch_us": 1e3 * k2ms / k2n,
+                                 "traffic": traffic_summary().get("fp64")}
+            else:
+                # step-wise: reset + three kernels per substep, from the step time
+                a2 = alg_bytes("fp64", n, na, ng) * args.substeps / (sum(ms2) / k2 / 1e3) / 1e9
+                d["roofline"] = {"achieved": a2, "frac": a2 / hbm, "from": "step time (4 launches per substep)"}
             extra[key] = d
             mm.gpu.close()
         extra["speedup_fp32_vs_fp64_stepwise"] = value / extra["fp64_stepwise"]["value"]
@@ -453,9 +473,10 @@ def main():
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sum(ms) / len(ms), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.form == "fp32" else "f64", "data": "synthetic",
             "config": {"workload": f"{name}: 2D MLS-MPM ice indentation, {n} particles, {p0.GridX}x{p0.GridY} grid "
-                                   f"(h = 1/{round(1 / p0.cellsize)} m), dt {p0.InitialTimeStep:g}, FP32 strain form",
+                                   f"(h = 1/{round(1 / p0.cellsize)} m), dt {p0.InitialTimeStep:g}, "
+                                   f"{'FP32 strain form' if args.form == 'fp32' else 'FP64 fused form'}",
                        "substeps_per_step": args.substeps, "tile": im.TILE_VARIANTS[tile], "threads": args.threads,
                        "tile_choice": tune_note, "active_nodes": na,
                        "l2": "flushed (256 MB write) before every timed step", "parallelism": f"replicas x{world}"},
