@@ -62,6 +62,24 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
+    """The largest x over all ranks (the job's time is its slowest
+    replica's); x itself without a process group."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, units_per_rank: float, seconds: float) -> float:
+    """Whole-job throughput of `world` replicas that each processed
+    units_per_rank units, timed by the slowest."""
+    return world * units_per_rank / seconds
+
+
 class Clocks:
     """Samples nvidia-smi every 200 ms while the timed region runs."""
 
@@ -242,12 +260,8 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def rank_max(x: float) -> float:
+        return max_over_ranks(x, dist, "cuda")
 
     name = args.config
     p0, soa0 = configs.make_scene(name)
@@ -308,8 +322,8 @@ def main():
     m = make(hform, tile)
     clocks = Clocks(local)
     ms, (kms, klaunch) = timed(m, args.steps, args.warmup, args.substeps, ktime=True, clocks=clocks)
-    total_s = max_over_ranks(sum(ms) / 1e3)
-    value = world * n * args.substeps * args.steps / total_s
+    total_s = rank_max(sum(ms) / 1e3)
+    value = job_rate(world, n * args.substeps * args.steps, total_s)
     redo = m.gpu.fp64_redo_count()
     m.gpu.close()
 
@@ -338,8 +352,8 @@ def main():
         for form, key in ((im.FORM_FP64, "fp64_fused"), (im.FORM_FP64_STEPWISE, "fp64_stepwise")):
             mm = make(form, tile64, threads64)
             ms2, (k2ms, k2n) = timed(mm, k2, 1, args.substeps, ktime=(form == im.FORM_FP64))
-            t2 = max_over_ranks(sum(ms2) / 1e3)
-            v2 = world * n * args.substeps * k2 / t2
+            t2 = rank_max(sum(ms2) / 1e3)
+            v2 = job_rate(world, n * args.substeps * k2, t2)
             d = {"value": v2, "ms_per_step": sum(ms2) / k2, "steps": k2,
                  "tile": im.TILE_VARIANTS[tile64] if form == im.FORM_FP64 else None,
                  "threads": threads64 if form == im.FORM_FP64 else None}
@@ -454,8 +468,8 @@ def main():
             g.synchronize()
             if k > 0:
                 times.append(g.elapsed_ms() / 1e3)
-        te = max_over_ranks(sum(times))
-        e2e = {"value": world * n * nsub * len(times) / te, "unit": UNIT, "h2d_bytes_per_step": bytes_soa,
+        te = rank_max(sum(times))
+        e2e = {"value": job_rate(world, n * nsub * len(times), te), "unit": UNIT, "h2d_bytes_per_step": bytes_soa,
                "d2h_bytes_per_step": d2h, "substeps_per_step": nsub, "steps": len(times),
                "what": "Model-level frame: H2D of the reference SoA from pinned memory, 10,000 substeps, "
                        "D2H of SoA + force bins + error word"}

@@ -1007,6 +1007,14 @@ extern "C" int icm_record_stop(icm_ctx *c)
     return ICM_OK;
 }
 
+extern "C" int icm_cycle_events(icm_ctx *c, void **start, void **stop)
+{
+    if (!c || !start || !stop) return icm::fail(ICM_ERR_ARG, "icm_cycle_events: null argument");
+    *start = (void *)c->ev_start;
+    *stop = (void *)c->ev_stop;
+    return ICM_OK;
+}
+
 extern "C" int icm_elapsed_ms(icm_ctx *c, float *ms)
 {
     if (!c || !ms) return icm::fail(ICM_ERR_ARG, "null argument");

@@ -169,6 +169,9 @@ int icm_stray_count(icm_ctx *ctx, unsigned long long *out);
 int icm_record_start(icm_ctx *ctx);
 int icm_record_stop(icm_ctx *ctx);
 int icm_elapsed_ms(icm_ctx *ctx, float *ms);
+/* The two events above as cudaEvent_t handles, for callers that record
+ * them themselves as model.cpp:19,30 does. */
+int icm_cycle_events(icm_ctx *ctx, void **start, void **stop);
 /* Per-launch timing of the fused substep kernel: when enabled, every
  * steady-state launch of icm_run_substeps is bracketed by a CUDA event pair
  * on the context's stream; icm_kernel_time returns the summed durations and
