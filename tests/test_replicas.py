@@ -38,7 +38,7 @@ def _replica(rank, world, port, out):
 
 def test_max_over_ranks_and_job_rate_gloo():
     world = 2
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.start_processes(_replica, args=(world, _free_port(), out), nprocs=world, start_method="spawn")
         res = dict(out)
