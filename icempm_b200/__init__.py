@@ -185,6 +185,12 @@ def _lib():
                 "icm_kernel_timing": (i, [vp, i]),
                 "icm_kernel_time": (i, [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
                 "icm_host_alloc": (i, [C.POINTER(vp), sz]), "icm_host_free": (i, [vp]),
+                "icm_cycle_events": (i, [vp, C.POINTER(vp), C.POINTER(vp)]),
+                "icm_save_snapshot": (i, [P, vp, vp, C.c_char_p, C.c_char_p, sz]),
+                "icm_read_snapshot_params": (i, [C.c_char_p, P]),
+                "icm_read_snapshot": (i, [C.c_char_p, vp, sz, vp, sz]),
+                "icm_save_pq": (i, [P, vp, C.c_char_p, C.c_char_p, sz]),
+                "icm_load_raw_points": (i, [P, C.c_char_p, vp, C.POINTER(C.c_int)]),
             }
             for name, (res, args) in sigs.items():
                 f = getattr(L, name)
@@ -475,15 +481,146 @@ class Model:
         if timed:
             g.record_start()
         n = p.UpdateEveryNthStep - (p.SimulationStep % p.UpdateEveryNthStep)
-        g.run_substeps(p, n)
+        # the frame advances a copy: the consumer of the previous frame may
+        # still read prms until the cycle lock is ours (model.cpp:32-45
+        # updates them after taking it)
+        nxt = SimParams.copy(p)
+        g.run_substeps(nxt, n)
         if timed:
             g.record_stop()
         self.processing_current_cycle_data.acquire()
+        p.SimulationStep, p.SimulationTime, p.indenter_x = nxt.SimulationStep, nxt.SimulationTime, nxt.indenter_x
         g.cuda_transfer_from_device()
         if not timed:
             self.compute_time_per_cycle = g.elapsed_ms() / p.UpdateEveryNthStep
         return p.SimulationTime < p.SimulationEndTime and not g.error_code
 
 
+def repitch_soa(src: np.ndarray, src_pitch: int, n: int, dst: np.ndarray, dst_pitch: int) -> None:
+    """Copies a particle SoA of n particles between pitches. Row 0 holds the
+    crushed bytes at byte i and the grain ids at byte src_pitch + 2i
+    (point.cpp:19-23), so it is moved field by field."""
+    s = src[: src_pitch * N_PTS_ARRAYS].reshape(N_PTS_ARRAYS, src_pitch)
+    d = dst[: dst_pitch * N_PTS_ARRAYS].reshape(N_PTS_ARRAYS, dst_pitch)
+    d[1:, :n] = s[1:, :n]
+    d[1:, n:] = 0
+    sb = s[0].view(np.uint8)
+    db = d[0].view(np.uint8)
+    db[:] = 0
+    db[:n] = sb[:n]
+    db[dst_pitch: dst_pitch + 2 * n] = sb[src_pitch: src_pitch + 2 * n]
+
+
+class SnapshotManager:
+    """Mirror of icy::SnapshotManager (snapshotmanager.h:15-31) over the
+    library's own HDF5 writer and reader."""
+
+    directory_snapshots = "snapshots"
+    directory_pq = "pq"
+
+    def __init__(self, model: Optional["Model"] = None):
+        self.model = model
+
+    def SaveSnapshot(self, outputDirectory: str) -> str:
+        """d%05d.h5 of the current frame (snapshotmanager.cpp:60-104);
+        returns the path written."""
+        m, g = self.model, self.model.gpu
+        out = C.create_string_buffer(4096)
+        _check(_lib().icm_save_snapshot(C.byref(m.prms), g.tmp_transfer_buffer.ctypes.data,
+                                        g.host_side_indenter_force_accumulator.ctypes.data,
+                                        os.fsencode(outputDirectory), out, len(out)))
+        return out.value.decode()
+
+    def ReadSnapshot(self, fileName: str) -> int:
+        """Resumes from a snapshot (the reference's ReadSnapshot,
+        snapshotmanager.cpp:145-184, is commented out): SimParams from the
+        file with this run's device buffers (re-allocated when the sizes
+        differ), the particle SoA uploaded, constants updated. Returns the
+        frame number."""
+        m, g = self.model, self.model.gpu
+        tmp = SimParams()
+        _check(_lib().icm_read_snapshot_params(os.fsencode(fileName), C.byref(tmp)))
+        src_pitch = int(tmp.nPtsPitch)
+        soa = np.empty(src_pitch * N_PTS_ARRAYS, dtype=np.float64)
+        bins = np.empty(2 * tmp.n_indenter_subdivisions, dtype=np.float64)
+        _check(_lib().icm_read_snapshot(os.fsencode(fileName), soa.ctypes.data, soa.size, bins.ctypes.data,
+                                        bins.size))
+        keep = {k: getattr(m.prms, k) for k in ("grid_array", "pts_array", "indenter_force_accumulator",
+                                                 "nPtsPitch", "nGridPitch")}
+        need_alloc = (not g.initialized or g.tmp_transfer_buffer is None or tmp.nPts > m.prms.nPts
+                      or tmp.GridX * tmp.GridY > m.prms.GridX * m.prms.GridY
+                      or tmp.n_indenter_subdivisions != m.prms.n_indenter_subdivisions)
+        C.memmove(C.byref(m.prms), C.byref(tmp), C.sizeof(SimParams))
+        if need_alloc:
+            g.cuda_allocate_arrays(tmp.GridX * tmp.GridY, tmp.nPts)
+        else:
+            for k, v in keep.items():
+                setattr(m.prms, k, v)
+        repitch_soa(soa, src_pitch, int(tmp.nPts), g.tmp_transfer_buffer, int(m.prms.nPtsPitch))
+        g.transfer_ponts_to_device()
+        g.host_side_indenter_force_accumulator[:] = bins
+        m.Prepare()
+        return int(m.prms.SimulationStep // max(m.prms.UpdateEveryNthStep, 1))
+
+    def LoadRawPoints(self, fileName: str) -> None:
+        """snapshotmanager.cpp:186-286: reads the point cloud, allocates,
+        uploads, Reset and Prepare."""
+        m, g = self.model, self.model.gpu
+        n = C.c_int(0)
+        _check(_lib().icm_load_raw_points(C.byref(m.prms), os.fsencode(fileName), None, C.byref(n)))
+        g.cuda_allocate_arrays(m.prms.GridTotal, n.value)
+        _check(_lib().icm_load_raw_points(C.byref(m.prms), os.fsencode(fileName), g.tmp_transfer_buffer.ctypes.data,
+                                          C.byref(n)))
+        g.transfer_ponts_to_device()
+        m.Reset()
+        m.Prepare()
+
+    def SavePQ(self, outputDirectory: str) -> str:
+        """pq%05d.h5 of the current frame (snapshotmanager.cpp:14-56)."""
+        m, g = self.model, self.model.gpu
+        out = C.create_string_buffer(4096)
+        _check(_lib().icm_save_pq(C.byref(m.prms), g.tmp_transfer_buffer.ctypes.data, os.fsencode(outputDirectory),
+                                  out, len(out)))
+        return out.value.decode()
+
+
+def load_raw_points_host(prms: SimParams, fileName: str) -> np.ndarray:
+    """LoadRawPoints into a host SoA only (no device): sets prms as the
+    loader does and returns the 16 x pitch SoA (pitch from pitch_elems)."""
+    n = C.c_int(0)
+    _check(_lib().icm_load_raw_points(C.byref(prms), os.fsencode(fileName), None, C.byref(n)))
+    prms.nPtsPitch = pitch_elems(n.value)
+    out = np.zeros(prms.nPtsPitch * N_PTS_ARRAYS, dtype=np.float64)
+    _check(_lib().icm_load_raw_points(C.byref(prms), os.fsencode(fileName), out.ctypes.data, C.byref(n)))
+    return out
+
+
+def save_snapshot_host(prms: SimParams, soa: np.ndarray, bins: np.ndarray, outputDirectory: str) -> str:
+    """SaveSnapshot from host buffers (prms.nPtsPitch must describe soa)."""
+    out = C.create_string_buffer(4096)
+    _check(_lib().icm_save_snapshot(C.byref(prms), soa.ctypes.data, bins.ctypes.data, os.fsencode(outputDirectory),
+                                    out, len(out)))
+    return out.value.decode()
+
+
+def read_snapshot_host(fileName: str):
+    """(SimParams, SoA, bins) of a snapshot file, host only."""
+    p = SimParams()
+    _check(_lib().icm_read_snapshot_params(os.fsencode(fileName), C.byref(p)))
+    soa = np.empty(int(p.nPtsPitch) * N_PTS_ARRAYS, dtype=np.float64)
+    bins = np.empty(2 * p.n_indenter_subdivisions, dtype=np.float64)
+    _check(_lib().icm_read_snapshot(os.fsencode(fileName), soa.ctypes.data, soa.size, bins.ctypes.data, bins.size))
+    return p, soa, bins
+
+
+def save_pq_host(prms: SimParams, soa: np.ndarray, outputDirectory: str) -> str:
+    """SavePQ from a host SoA."""
+    out = C.create_string_buffer(4096)
+    _check(_lib().icm_save_pq(C.byref(prms), soa.ctypes.data, os.fsencode(outputDirectory), out, len(out)))
+    return out.value.decode()
+
+
 __all__ = ["SimParams", "BlockDesc", "GPU_Implementation5", "Model", "SoA", "make_block", "pitch_elems", "library",
+           "SnapshotManager", "repitch_soa", "load_raw_points_host", "save_snapshot_host", "read_snapshot_host",
+           "save_pq_host",
            "FORM_FP64_STEPWISE", "FORM_FP64", "FORM_FP32", "FORM_NAMES", "TILE_VARIANTS", "LIB_PATH"]

@@ -25,7 +25,7 @@ ORACLE = os.path.join(ROOT, "oracle")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["device_layer.cu", "noalloc.cu"]
-CPP_SOURCES = ["params.cpp", "scene.cpp", "errors.cpp", "snapshot.cpp"]
+CPP_SOURCES = ["params.cpp", "scene.cpp", "errors.cpp", "snapshot.cpp", "hdf5_lite.cpp"]
 
 
 def _deps():
@@ -58,7 +58,7 @@ def build_lib(force: bool = False) -> str:
     if not force and not _stale(LIB, _deps()):
         return LIB
     cmd = ["nvcc", *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-o", LIB + ".tmp", *srcs]
+           "-o", LIB + ".tmp", *srcs, "-lz"]
     _run(cmd)
     os.replace(LIB + ".tmp", LIB)
     return LIB
@@ -66,12 +66,12 @@ def build_lib(force: bool = False) -> str:
 
 def build_cli(force: bool = False) -> str:
     """Builds the C++ driver against libicempm.so."""
-    src = os.path.join(ROOT, "cli", "cm.cpp")
+    src = os.path.join(PKG, "cli", "cm.cpp")
     if not os.path.exists(src):
         return ""
     if not force and not _stale(CLI, _deps() + [src, LIB]):
         return CLI
-    cmd = ["g++", "-O2", "-std=c++17", "-pthread", "-I", os.path.join(ROOT, "include"), src,
+    cmd = ["g++", "-O2", "-std=c++17", "-pthread", "-Wall", "-I", os.path.join(ROOT, "include"), src,
            "-L", PKG, "-licempm", "-Wl,-rpath,$ORIGIN", "-o", CLI]
     _run(cmd)
     return CLI

@@ -2,13 +2,11 @@
 // SnapshotManager::LoadRawPoints (simulation/snapshotmanager.cpp:186-286)
 // when no HDF5 point cloud is used.
 //
-// The point pipeline of LoadRawPoints is kept: raw points are float32
-// (Points_Raw_2D is read as NATIVE_FLOAT, :202-204), sorted by grid cell with
-// the SortPoints key (int)(x/h-0.5) + (int)(y/h-0.5)*GridX (:288-304; a
-// stable sort here, so equal keys keep generation order), centred in x and
-// lifted by 2h in float arithmetic (:244-250, :275-276), then widened to
-// double. Volume, bounding box, ParticleVolume = Volume/N and
-// ParticleMass = rho * ParticleVolume follow :225-242 and :267-268.
+// The point pipeline of LoadRawPoints is kept (points.h): float32 raw
+// points, sorted by grid cell, centred in x and lifted by 2h in float
+// arithmetic, then widened to double. Volume = block area, ParticleVolume =
+// Volume/N and ParticleMass = rho * ParticleVolume follow :225-242 and
+// :267-268.
 // Deviation (documented): the indenter starts just touching the block's left
 // face, x = block_left - r, at an explicit height above the block bottom,
 // instead of the IndDepth-based placement of :253-265.
@@ -21,6 +19,7 @@
 
 #include "../../include/icempm.h"
 #include "errors.h"
+#include "points.h"
 
 namespace {
 
@@ -39,8 +38,7 @@ extern "C" int icm_scene_block(icy_SimParams *p, const icm_block_desc *d, double
     if (n_out) *n_out = (int)n;
 
     std::mt19937_64 rng(d->seed);
-    struct Raw { float x, y; short g; };
-    std::vector<Raw> pts((size_t)n);
+    std::vector<icm::RawPoint> pts((size_t)n);
     size_t k = 0;
     for (int cy = 0; cy < d->cells_y; cy++)
         for (int cx = 0; cx < d->cells_x; cx++)
@@ -92,33 +90,13 @@ extern "C" int icm_scene_block(icy_SimParams *p, const icm_block_desc *d, double
         q.g = (short)arg;
     }
 
-    if (p->SortPointsByGridCell) {
-        const double hinv = p->cellsize_inv;
-        const int gx = p->GridX;
-        std::stable_sort(pts.begin(), pts.end(), [hinv, gx](const Raw &a, const Raw &b) {
-            int ai = (int)(a.x * hinv - 0.5) + ((int)(a.y * hinv - 0.5)) * gx;
-            int bi = (int)(b.x * hinv - 0.5) + ((int)(b.y * hinv - 0.5)) * gx;
-            return ai < bi;
-        });
-    }
+    if (p->SortPointsByGridCell) icm::sort_points(*p, pts);
 
-    p->nPts = (int)n;
+    const icm::Placement pl = icm::place_points(p, pts);
     p->Volume = (double)(float)(W * Hb);
-    auto mmx = std::minmax_element(pts.begin(), pts.end(), [](const Raw &a, const Raw &b) { return a.x < b.x; });
-    p->xmin = mmx.first->x;
-    p->xmax = mmx.second->x;
-    const float length = (float)(p->xmax - p->xmin);
-    auto mmy = std::minmax_element(pts.begin(), pts.end(), [](const Raw &a, const Raw &b) { return a.y < b.y; });
-    p->ymin = mmy.first->y;
-    p->ymax = mmy.second->y;
-    icm_params_compute_block_coords(p);
-
-    const double box_x = p->GridX * h;
-    const double x_offset = (box_x - length) / 2;
-    const double y_offset = 2 * h;
     const double r = p->IndDiameter / 2;
-    const double block_left = p->xmin + x_offset;
-    const double block_bottom = p->ymin + y_offset;
+    const double block_left = p->xmin + pl.x_offset;
+    const double block_bottom = p->ymin + pl.y_offset;
     p->indenter_x = block_left - r;
     p->indenter_y = block_bottom + d->ind_y_above_floor;
     p->indenter_x_initial = p->indenter_x;
@@ -126,23 +104,6 @@ extern "C" int icm_scene_block(icy_SimParams *p, const icm_block_desc *d, double
     p->ParticleVolume = p->Volume / (double)n;
     p->ParticleMass = p->ParticleVolume * p->Density;
 
-    if (host_soa) {
-        const size_t pitch = icm_pitch_elems((size_t)n);
-        std::memset(host_soa, 0, sizeof(double) * pitch * ICM_N_PTS_ARRAYS);
-        uint8_t *crushed = (uint8_t *)host_soa;
-        short *grain = (short *)((char *)host_soa + pitch);
-        for (long i = 0; i < n; i++) {
-            float fx = pts[(size_t)i].x, fy = pts[(size_t)i].y;
-            fx = (float)(fx + x_offset);
-            fy = (float)(fy + y_offset);
-            crushed[i] = 0;
-            grain[i] = pts[(size_t)i].g;
-            host_soa[(size_t)ICM_IDX_JP_INV * pitch + i] = 1.0;
-            host_soa[(size_t)ICM_IDX_POSX * pitch + i] = fx;
-            host_soa[(size_t)(ICM_IDX_POSX + 1) * pitch + i] = fy;
-            host_soa[(size_t)ICM_IDX_FE00 * pitch + i] = 1.0;
-            host_soa[(size_t)(ICM_IDX_FE00 + 3) * pitch + i] = 1.0;
-        }
-    }
+    if (host_soa) icm::fill_soa(pts, pl, host_soa, icm_pitch_elems((size_t)n));
     return ICM_OK;
 }

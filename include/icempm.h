@@ -199,6 +199,34 @@ void *icm_stream(icm_ctx *ctx);
  * looks up the scratch's device address; make that first call before any
  * stream capture. */
 int icm_run_substeps_noalloc(icy_SimParams *p, double *pts, double *bins, int *err, int n, void *stream);
+/* ------------------------------------------------------------ snapshots
+ * SnapshotManager (simulation/snapshotmanager.cpp) on the library's own
+ * HDF5 reader and writer (no libhdf5); host-side, no device calls. Files
+ * are numbered by the frame SimulationStep / UpdateEveryNthStep
+ * (parameters_sim.h:88); path_out (may be NULL) receives the file written. */
+/* SaveSnapshot (:60-104): <dir>/snapshots/d%05d.h5 with Indenter_2D
+ * (f64[2*n_indenter_subdivisions]), Params (bitfield bytes[432], the
+ * SimParams bytes, with the 14 attributes of SaveParametersAsAttributes
+ * :106-142) and Points (f64[16*nPtsPitch], the particle SoA). */
+int icm_save_snapshot(const icy_SimParams *p, const double *host_soa, const double *host_bins, const char *dir,
+                      char *path_out, size_t cap);
+/* Reading a snapshot back to resume a run (the reference's ReadSnapshot,
+ * :145-184, is commented out): the stored SimParams (its device pointers
+ * are the writer's and must be replaced), then the particle SoA (soa_elems
+ * = 16*nPtsPitch) and force bins (host_bins may be NULL). */
+int icm_read_snapshot_params(const char *path, icy_SimParams *out);
+int icm_read_snapshot(const char *path, double *host_soa, size_t soa_elems, double *host_bins, size_t bins_elems);
+/* SavePQ (:14-56): <dir>/pq/pq%05d.h5 with PQ_intact and PQ_crushed
+ * (f64[n,2] of the P and Q rows, split by the crushed byte); PQ_intact
+ * carries the parameter attributes. */
+int icm_save_pq(const icy_SimParams *p, const double *host_soa, const char *dir, char *path_out, size_t cap);
+/* LoadRawPoints (:186-286) + SortPoints (:288-304): reads Points_Raw_2D
+ * (float[N,2]), GrainIDs (int16[N]) and its attribute volume (float), sorts
+ * by grid cell when SortPointsByGridCell (stable sort), sets nPts, Volume,
+ * the bounding box, the indenter start from IndDepth/SetupType,
+ * ParticleVolume and ParticleMass, and returns N. With host_soa non-NULL
+ * (after icm_allocate_arrays has set nPtsPitch) it also fills the SoA. */
+int icm_load_raw_points(icy_SimParams *p, const char *path, double *host_soa, int *n_out);
 /* Pinned host memory for transfer buffers (cudaMallocHost/cudaFreeHost). */
 int icm_host_alloc(void **ptr, size_t bytes);
 int icm_host_free(void *ptr);

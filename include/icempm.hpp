@@ -13,6 +13,7 @@
  *                        icm_last_error() on a non-zero status, as the
  *                        reference members throw on CUDA errors
  *   icy::Model           model.h:26-52, model.cpp:11-67
+ *   icy::SnapshotManager snapshotmanager.h:15-31 (HDF5 without libhdf5)
  *
  * Extensions (no counterpart in the reference): GPU_Implementation5::
  * set_form / set_tile / run_substeps select and run the fused forms;
@@ -24,6 +25,7 @@
 #define ICEMPM_HPP
 
 #include <array>
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
 #include <functional>
@@ -31,6 +33,7 @@
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "icempm.h"
 
@@ -101,6 +104,33 @@ struct Point {
     }
 };
 
+/* The cycle lock of model.h:42. The simulation thread takes it before a
+ * frame's copy to the host and the thread that consumes the frame releases
+ * it (cli/main.cpp:51-62), so it is a binary semaphore rather than a
+ * std::mutex, which the locking thread alone may unlock. */
+class CycleLock {
+public:
+    void lock()
+    {
+        std::unique_lock<std::mutex> l(m_);
+        cv_.wait(l, [&] { return !held_; });
+        held_ = true;
+    }
+    void unlock()
+    {
+        {
+            std::lock_guard<std::mutex> l(m_);
+            held_ = false;
+        }
+        cv_.notify_all();
+    }
+
+private:
+    std::mutex m_;
+    std::condition_variable cv_;
+    bool held_ = false;
+};
+
 class Model;
 
 }  // namespace icy
@@ -169,6 +199,7 @@ public:
         icy::icm_check(icm_set_tile(ctx_, variant, threads));
     }
     inline void run_substeps(int n);
+    void run_substeps(icy_SimParams &p, int n) { icy::icm_check(icm_run_substeps(ctx_, &p, n)); }
     icm_ctx *context() const { return ctx_; }
 
 private:
@@ -208,9 +239,16 @@ public:
         const bool timed = prms.SimulationStep % (prms.UpdateEveryNthStep * 2) == 0;
         gpu.cuda_reset_indenter_force_accumulator();
         if (timed) icm_check(icm_record_start(gpu.context()));
-        gpu.run_substeps(n);
+        // the frame advances a copy: the consumer of the previous frame may
+        // still read prms until the cycle lock is ours (model.cpp:32-45
+        // updates them after taking it)
+        icy_SimParams next = prms;
+        gpu.run_substeps(next, n);
         if (timed) icm_check(icm_record_stop(gpu.context()));
         processing_current_cycle_data.lock();  // held until the host has consumed the frame
+        prms.SimulationStep = next.SimulationStep;
+        prms.SimulationTime = next.SimulationTime;
+        prms.indenter_x = next.indenter_x;
         gpu.cuda_transfer_from_device();
         if (!timed) {
             float ms = 0;
@@ -224,11 +262,87 @@ public:
     icy::SimParams prms;
     GPU_Implementation5 gpu;
     float compute_time_per_cycle = 0;
-    std::mutex processing_current_cycle_data;
+    icy::CycleLock processing_current_cycle_data;
 
 private:
     bool abortRequested = false;
 };
+
+/* icy::SnapshotManager (snapshotmanager.h:15-31) over the library's HDF5
+ * code. ReadSnapshot resumes a run (the reference's is commented out). */
+namespace icy {
+class SnapshotManager {
+public:
+    icy::Model *model = nullptr;
+    const std::string directory_snapshots = "snapshots";
+    const std::string directory_pq = "pq";
+
+    std::string SaveSnapshot(std::string outputDirectory)
+    {
+        char path[4096];
+        icm_check(icm_save_snapshot(&model->prms, model->gpu.tmp_transfer_buffer,
+                                    model->gpu.host_side_indenter_force_accumulator, outputDirectory.c_str(), path,
+                                    sizeof(path)));
+        return path;
+    }
+    std::string SavePQ(std::string outputDirectory)
+    {
+        char path[4096];
+        icm_check(icm_save_pq(&model->prms, model->gpu.tmp_transfer_buffer, outputDirectory.c_str(), path,
+                              sizeof(path)));
+        return path;
+    }
+    void LoadRawPoints(std::string fileName)
+    {
+        int n = 0;
+        icm_check(icm_load_raw_points(&model->prms, fileName.c_str(), nullptr, &n));
+        model->gpu.cuda_allocate_arrays((size_t)model->prms.GridX * model->prms.GridY, (size_t)n);
+        icm_check(icm_load_raw_points(&model->prms, fileName.c_str(), model->gpu.tmp_transfer_buffer, &n));
+        model->gpu.transfer_ponts_to_device();
+        model->Reset();
+        model->Prepare();
+    }
+    /* Returns the frame number of the snapshot. */
+    int ReadSnapshot(std::string fileName)
+    {
+        icy_SimParams tmp;
+        icm_check(icm_read_snapshot_params(fileName.c_str(), &tmp));
+        const size_t src_pitch = tmp.nPtsPitch, n = (size_t)tmp.nPts;
+        std::vector<double> soa(src_pitch * SimParams::nPtsArrays), bins(2 * (size_t)tmp.n_indenter_subdivisions);
+        icm_check(icm_read_snapshot(fileName.c_str(), soa.data(), soa.size(), bins.data(), bins.size()));
+        SimParams &p = model->prms;
+        const bool realloc = !model->gpu.tmp_transfer_buffer || tmp.nPts > p.nPts ||
+                             (size_t)tmp.GridX * tmp.GridY > (size_t)p.GridX * p.GridY ||
+                             tmp.n_indenter_subdivisions != p.n_indenter_subdivisions;
+        icy_SimParams keep = p;
+        static_cast<icy_SimParams &>(p) = tmp;
+        if (realloc) {
+            model->gpu.cuda_allocate_arrays((size_t)tmp.GridX * tmp.GridY, n);
+        } else {
+            p.grid_array = keep.grid_array;
+            p.pts_array = keep.pts_array;
+            p.indenter_force_accumulator = keep.indenter_force_accumulator;
+            p.nPtsPitch = keep.nPtsPitch;
+            p.nGridPitch = keep.nGridPitch;
+        }
+        // the utility row holds crushed bytes at byte i and grain ids at
+        // byte pitch + 2i (point.cpp:19-23): move it field by field
+        const size_t dst_pitch = p.nPtsPitch;
+        double *dst = model->gpu.tmp_transfer_buffer;
+        std::memset(dst, 0, sizeof(double) * dst_pitch * SimParams::nPtsArrays);
+        for (size_t r = 1; r < SimParams::nPtsArrays; r++)
+            std::memcpy(dst + r * dst_pitch, soa.data() + r * src_pitch, sizeof(double) * n);
+        const char *s0 = reinterpret_cast<const char *>(soa.data());
+        char *d0 = reinterpret_cast<char *>(dst);
+        std::memcpy(d0, s0, n);
+        std::memcpy(d0 + dst_pitch, s0 + src_pitch, 2 * n);
+        model->gpu.transfer_ponts_to_device();
+        std::memcpy(model->gpu.host_side_indenter_force_accumulator, bins.data(), sizeof(double) * bins.size());
+        model->Prepare();
+        return p.UpdateEveryNthStep > 0 ? p.SimulationStep / p.UpdateEveryNthStep : 0;
+    }
+};
+}  // namespace icy
 
 inline void GPU_Implementation5::cuda_update_constants()
 {
