@@ -24,7 +24,7 @@ CLI = os.path.join(PKG, "cm")
 ORACLE = os.path.join(ROOT, "oracle")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["device_layer.cu", "noalloc.cu"]
+CU_SOURCES = ["device_layer.cu", "noalloc.cu", "mlp.cu"]
 CPP_SOURCES = ["params.cpp", "scene.cpp", "errors.cpp", "snapshot.cpp", "hdf5_lite.cpp"]
 
 

@@ -141,32 +141,30 @@ __device__ __forceinline__ bool outside_failure_surface64(const icy_SimParams &P
     return yv > 0;
 }
 
-// ComputePQ + failure check + Drucker-Prager map on the advected Fe.
-// Updates Fe, Jp_inv and crushed in place; returns p_tr, q_tr.
-__device__ __forceinline__ void constitutive64(const icy_SimParams &P, M2d &Fe, double &Jp_inv,
-                                               uint8_t &crushed, GrainRes grain, double &p_tr, double &q_tr)
+// Drucker-Prager projection of a crushed particle in principal space
+// (Wolper_Drucker_Prager, gpu_implementation5.cu:48-94): from the trial
+// singular values s0 >= s1 and Jp_inv, the new singular values and Jp_inv.
+// changed = false when the state is left as it is (inside the yield surface).
+struct DpResult { bool changed; double s0, s1, jp; };
+
+__device__ __forceinline__ DpResult dp_project64(const icy_SimParams &P, double s0, double s1, double Jp_inv)
 {
     const double mu = P.mu, kappa = P.kappa;
-    Svd64 d = svd2x2_64(Fe);
-    double Je_tr = d.s0 * d.s1;
-    p_tr = -(kappa / 2.) * (Je_tr * Je_tr - 1.);
-    double sq0 = d.s0 * d.s0, sq1 = d.s1 * d.s1;
-    double half_sum = (sq0 + sq1) / 2;
-    double f = mu / Je_tr;
-    double sh0 = f * (sq0 - half_sum), sh1 = f * (sq1 - half_sum);
-    q_tr = kCoeff1 * sqrt(sh0 * sh0 + sh1 * sh1);
-
-    if (crushed == 0 && outside_failure_surface64(P, grain, p_tr, q_tr)) crushed = 1;
-    if (crushed != 1) return;
-
+    const double Je_tr = s0 * s1;
+    const double p_tr = -(kappa / 2.) * (Je_tr * Je_tr - 1.);
+    const double sq0 = s0 * s0, sq1 = s1 * s1;
+    const double half_sum = (sq0 + sq1) / 2;
+    const double f = mu / Je_tr;
+    const double sh0 = f * (sq0 - half_sum), sh1 = f * (sq1 - half_sum);
+    const double q_tr = kCoeff1 * sqrt(sh0 * sh0 + sh1 * sh1);
     const double tan_phi = P.DP_tan_phi, p_thr = P.DP_threshold_p;
     const double pmax = P.IceCompressiveStrength, qmax = P.IceShearStrength;
+    DpResult r{false, s0, s1, Jp_inv};
     if (p_tr < -p_thr || Jp_inv < 1) {
         double p_new = -p_thr;
         double Je_new = sqrt(-2. * p_new / kappa + 1.);
         double sn = sqrt(Je_new);
-        Fe = usvt64(d, sn, sn);
-        Jp_inv *= Je_new / Je_tr;
+        r = {true, sn, sn, Jp_inv * (Je_new / Je_tr)};
     } else {
         double q_n_1;
         if (p_tr > pmax) {
@@ -186,8 +184,34 @@ __device__ __forceinline__ void constitutive64(const icy_SimParams &P, M2d &Fe, 
             }
             double ff = s_hat_n_1_norm * (Je_tr / mu);
             double mean = (sq0 + sq1) / 2.0;
-            Fe = usvt64(d, sqrt(ff * n0 + mean), sqrt(ff * n1 + mean));
+            r = {true, sqrt(ff * n0 + mean), sqrt(ff * n1 + mean), Jp_inv};
         }
+    }
+    return r;
+}
+
+// ComputePQ + failure check + Drucker-Prager map on the advected Fe.
+// Updates Fe, Jp_inv and crushed in place; returns p_tr, q_tr.
+__device__ __forceinline__ void constitutive64(const icy_SimParams &P, M2d &Fe, double &Jp_inv,
+                                               uint8_t &crushed, GrainRes grain, double &p_tr, double &q_tr)
+{
+    const double mu = P.mu, kappa = P.kappa;
+    Svd64 d = svd2x2_64(Fe);
+    double Je_tr = d.s0 * d.s1;
+    p_tr = -(kappa / 2.) * (Je_tr * Je_tr - 1.);
+    double sq0 = d.s0 * d.s0, sq1 = d.s1 * d.s1;
+    double half_sum = (sq0 + sq1) / 2;
+    double f = mu / Je_tr;
+    double sh0 = f * (sq0 - half_sum), sh1 = f * (sq1 - half_sum);
+    q_tr = kCoeff1 * sqrt(sh0 * sh0 + sh1 * sh1);
+
+    if (crushed == 0 && outside_failure_surface64(P, grain, p_tr, q_tr)) crushed = 1;
+    if (crushed != 1) return;
+
+    const DpResult r = dp_project64(P, d.s0, d.s1, Jp_inv);
+    if (r.changed) {
+        Fe = usvt64(d, r.s0, r.s1);
+        Jp_inv = r.jp;
     }
 }
 

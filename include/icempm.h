@@ -199,6 +199,36 @@ void *icm_stream(icm_ctx *ctx);
  * looks up the scratch's device address; make that first call before any
  * stream capture. */
 int icm_run_substeps_noalloc(icy_SimParams *p, double *pts, double *bins, int *err, int n, void *stream);
+/* ------------------------------------------------ learned projection
+ * No counterpart in the reference. A 6 -> 64 -> 64 -> 3 GELU network
+ * (BF16 weights, FP32 accumulation) predicts the Drucker-Prager projection
+ * of a crushed particle (Wolper_Drucker_Prager, gpu_implementation5.cu:
+ * 48-94) in principal space from its trial singular values and Jp_inv.
+ * Parameters are icm_mlp_floats() floats: W1[64][6], b1[64], W2[64][64],
+ * b2[64], W3[3][64], b3[3], then the input/output normalisation x_mu[6],
+ * x_sd[6], y_mu[3], y_sd[3]. */
+int icm_mlp_floats(void);
+/* Sets the normalisation part of net from n samples (x: n x 6, y: n x 3). */
+int icm_mlp_normalise(float *net, const float *x, const float *y, int n);
+typedef struct icm_mlp_train_cfg {
+    int steps;        /* Adam steps */
+    int batch_tiles;  /* batch = 128 * batch_tiles samples, drawn at random each step */
+    float lr;         /* peak learning rate (cosine decay to lr/20) */
+    uint32_t seed;
+} icm_mlp_train_cfg;
+/* Trains net (in place; start from caller-initialised weights) on the
+ * tensor cores of `device`; loss_hist (may be NULL) receives the mean
+ * squared error of each step on normalised targets. */
+int icm_mlp_train(int device, const float *x, const float *y, int n, const icm_mlp_train_cfg *cfg, float *net,
+                  float *loss_hist);
+/* Gradient of the mean squared error over the n samples (one forward and
+ * backward pass of the training kernel) in the parameter layout, and the
+ * loss. */
+int icm_mlp_gradient(int device, const float *net, const float *x, const float *y, int n, float *grad, float *loss);
+/* Network outputs (denormalised, n x 3) for n inputs: the tensor-core
+ * batch form (warp_form = 0) or the warp form the substep uses (1). */
+int icm_mlp_infer(int device, const float *net, const float *x, int n, float *y, int warp_form);
+
 /* ------------------------------------------------------------ snapshots
  * SnapshotManager (simulation/snapshotmanager.cpp) on the library's own
  * HDF5 reader and writer (no libhdf5); host-side, no device calls. Files
