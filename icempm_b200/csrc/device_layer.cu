@@ -108,6 +108,16 @@ struct icm_ctx {
     unsigned long long *d_redo = nullptr;
     unsigned long long *d_strays = nullptr;
 
+    // surrogate form: device copy of the network, tolerance, {accepted, exact}
+    MlpWarpNet *d_mlp = nullptr;
+    float mlp_tol = 0.02f;
+    unsigned long long *d_mlp_counts = nullptr;
+    // harvest of crushed particles' trial states (6 floats each)
+    float *d_harvest = nullptr;
+    unsigned *d_harvest_n = nullptr;
+    unsigned harvest_cap = 0;
+    int harvest_every = 0;
+
     // optional per-launch timing of the fused substep kernel (kModeFull)
     bool ktime = false;
     std::vector<cudaEvent_t> kev;  // pairs
@@ -123,6 +133,9 @@ struct icm_ctx {
 };
 
 // ------------------------------------------------------------ helpers
+
+// the internal storage of a form: the surrogate form keeps FP32 state
+static int storage_form(int form) { return form == ICM_FORM_FP32_SURROGATE ? ICM_FORM_FP32 : form; }
 
 static int check_params(icm_ctx *c, const icy_SimParams *p)
 {
@@ -156,7 +169,7 @@ static icy_SimParams kernel_params(icm_ctx *c, const icy_SimParams *p)
 
 static Consts32 make_consts32(const icy_SimParams &P)
 {
-    Consts32 k;
+    Consts32 k{};
     k.h = (float)P.cellsize;
     k.h_inv = (float)P.cellsize_inv;
     k.dt = (float)P.InitialTimeStep;
@@ -324,7 +337,7 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
     geometry(P, c->tile_variant, g, ntiles);
     const size_t ncells = (size_t)ntiles * g.TX * g.TY;
     if (ncells > (size_t)kScanChunk * kScanChunk) return icm::fail(ICM_ERR_ARG, "grid too large for the binning scan");
-    int rc = ensure_grids(c, c->form, (size_t)P.nPts, (size_t)P.GridX * P.GridY, (size_t)ntiles, ncells);
+    int rc = ensure_grids(c, storage_form(c->form), (size_t)P.nPts, (size_t)P.GridX * P.GridY, (size_t)ntiles, ncells);
     if (rc) return rc;
     cudaStream_t s = c->stream;
     const int n = P.nPts;
@@ -350,10 +363,10 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
     int nslots = 0;
     ICM_CUDA(cudaMemcpyAsync(&nslots, c->bin.group_base + ngroups, sizeof(int), cudaMemcpyDeviceToHost, s));
     ICM_CUDA(cudaStreamSynchronize(s));
-    if ((rc = ensure_slots(c, c->form, (size_t)std::max(nslots, 1)))) return rc;
+    if ((rc = ensure_slots(c, storage_form(c->form), (size_t)std::max(nslots, 1)))) return rc;
     ICM_CUDA(cudaMemsetAsync(c->bin.pid, 0xff, sizeof(int) * (size_t)std::max(nslots, 1), s));
     if (n > 0) {
-        if (c->form == ICM_FORM_FP64)
+        if (storage_form(c->form) == ICM_FORM_FP64)
             k_pack64<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.key, c->bin.cell_start, c->bin.group_base,
                                                      c->bin.pid, c->fz.p64);
         else
@@ -578,7 +591,9 @@ static int tile_order(icm_ctx *c, int ntiles, const int *&order)
 static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
 {
     icy_SimParams P = kernel_params(c, p);
-    if (!c->internal_valid || c->fz.form != c->form || c->internal_variant != c->tile_variant) {
+    if (c->form == ICM_FORM_FP32_SURROGATE && !c->d_mlp)
+        return icm::fail(ICM_ERR_STATE, "surrogate form without a network (icm_set_surrogate)");
+    if (!c->internal_valid || c->fz.form != storage_form(c->form) || c->internal_variant != c->tile_variant) {
         int rc = ensure_ref(c);
         if (rc) return rc;
         if ((rc = pack(c, P))) return rc;
@@ -587,7 +602,7 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     int ntiles;
     geometry(P, c->tile_variant, g, ntiles);
     const size_t nnodes = (size_t)P.GridX * P.GridY;
-    const size_t node_bytes = (c->form == ICM_FORM_FP64) ? sizeof(Node64) : sizeof(float4);
+    const size_t node_bytes = (storage_form(c->form) == ICM_FORM_FP64) ? sizeof(Node64) : sizeof(float4);
     cudaStream_t s = c->stream;
     for (int b = 0; b < 3; b++) ICM_CUDA(cudaMemsetAsync(c->fz.grid[b], 0, node_bytes * nnodes, s));
     ICM_CUDA(cudaMemsetAsync(c->fz.dirty, 0, 3 * (size_t)ntiles, s));
@@ -614,7 +629,11 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     R.cost = c->fz.cost;
     if ((rc = tile_order(c, ntiles, R.order))) return rc;
 
-    const Consts32 K32 = make_consts32(P);
+    Consts32 K32 = make_consts32(P);
+    K32.mlp = c->d_mlp;
+    K32.mlp_tol = c->mlp_tol;
+    K32.mlp_counts = c->d_mlp_counts;
+    bool harvest_now = false;  // this launch appends crushed particles' trial states
     const Pol64::Consts K64{0};
     auto launch = [&](int mode) -> int {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -630,8 +649,19 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
             e1 = c->kev[c->kev_used++];
             ICM_CUDA(cudaEventRecord(e0, c->stream));
         }
-        int r = (c->form == ICM_FORM_FP64) ? launch_variant<Pol64>(c, mode, ntiles, P, K64, c->fz.p64, R)
-                                           : launch_variant<Pol32>(c, mode, ntiles, P, K32, c->fz.p32, R);
+        int r;
+        if (c->form == ICM_FORM_FP64) {
+            r = launch_variant<Pol64>(c, mode, ntiles, P, K64, c->fz.p64, R);
+        } else {
+            Consts32 K = K32;
+            if (c->d_harvest && harvest_now) {
+                K.harvest = c->d_harvest;
+                K.harvest_n = c->d_harvest_n;
+                K.harvest_cap = c->harvest_cap;
+            }
+            r = (c->form == ICM_FORM_FP32_SURROGATE) ? launch_variant<Pol32S>(c, mode, ntiles, P, K, c->fz.p32, R)
+                                                     : launch_variant<Pol32>(c, mode, ntiles, P, K, c->fz.p32, R);
+        }
         if (e1) ICM_CUDA(cudaEventRecord(e1, c->stream));
         return r;
     };
@@ -654,6 +684,7 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
         R.force_slot = c->d_hist + 2 * (size_t)sidx;
         R.record_pq = ((p->SimulationStep + k) % p->UpdateEveryNthStep == 0) ? 1 : 0;
         any_pq |= R.record_pq != 0;
+        harvest_now = c->harvest_every > 0 && (p->SimulationStep + k) % c->harvest_every == 0;
         if ((rc = launch(k < n ? kModeFull : kModeFinal))) return rc;
         if (k < n && c->rebin_interval > 0 && k % c->rebin_interval == 0) {
             if ((rc = rebin_internal(c, P, c->internal_pq || any_pq))) return rc;
@@ -741,6 +772,7 @@ extern "C" int icm_destroy(icm_ctx *c)
     free_fused(c);
     free_binning(c);
     dfree(c->d_pts); dfree(c->d_grid); dfree(c->d_bins); dfree(c->d_err); dfree(c->d_hist); dfree(c->d_redo); dfree(c->d_strays);
+    dfree(c->d_mlp); dfree(c->d_mlp_counts); dfree(c->d_harvest); dfree(c->d_harvest_n);
     for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
     if (c->ev_start) cudaEventDestroy(c->ev_start);
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
@@ -752,7 +784,7 @@ extern "C" int icm_destroy(icm_ctx *c)
 extern "C" int icm_set_form(icm_ctx *c, int form)
 {
     if (!c) return icm::fail(ICM_ERR_ARG, "null context");
-    if (form < ICM_FORM_FP64_STEPWISE || form > ICM_FORM_FP32) return icm::fail(ICM_ERR_ARG, "unknown form");
+    if (form < ICM_FORM_FP64_STEPWISE || form > ICM_FORM_FP32_SURROGATE) return icm::fail(ICM_ERR_ARG, "unknown form");
     if (form == c->form) return ICM_OK;
     if (c->d_pts) {
         int rc = ensure_ref(c);
@@ -1060,6 +1092,95 @@ extern "C" int icm_kernel_time(icm_ctx *c, double *total_ms, long long *launches
 }
 
 extern "C" void *icm_stream(icm_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+// ------------------------------------------------ learned projection
+
+namespace icm {
+int mlp_prepare_warp_net(const float *host_net, MlpWarpNet **out);
+int mlp_label(const icy_SimParams &P, const float *d_harvest, int n, float *d_x, float *d_y, cudaStream_t s);
+}  // namespace icm
+
+extern "C" int icm_set_surrogate(icm_ctx *c, const float *net, float tolerance)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    if (net && !(tolerance > 0)) return icm::fail(ICM_ERR_ARG, "icm_set_surrogate: tolerance must be positive");
+    ICM_CUDA(cudaSetDevice(c->device));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    dfree(c->d_mlp);
+    if (!net) return ICM_OK;
+    int rc = mlp_prepare_warp_net(net, &c->d_mlp);
+    if (rc) return rc;
+    if (!c->d_mlp_counts && (rc = dalloc(&c->d_mlp_counts, 2))) return rc;
+    ICM_CUDA(cudaMemset(c->d_mlp_counts, 0, 2 * sizeof(unsigned long long)));
+    c->mlp_tol = tolerance;
+    return ICM_OK;
+}
+
+extern "C" int icm_surrogate_counts(icm_ctx *c, unsigned long long *accepted, unsigned long long *exact)
+{
+    if (!c || !accepted || !exact) return icm::fail(ICM_ERR_ARG, "icm_surrogate_counts: null argument");
+    unsigned long long h[2] = {0, 0};
+    if (c->d_mlp_counts) {
+        ICM_CUDA(cudaStreamSynchronize(c->stream));
+        ICM_CUDA(cudaMemcpy(h, c->d_mlp_counts, sizeof(h), cudaMemcpyDeviceToHost));
+    }
+    *accepted = h[0];
+    *exact = h[1];
+    return ICM_OK;
+}
+
+extern "C" int icm_set_harvest(icm_ctx *c, int capacity, int every)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    if (capacity < 0 || every < 0) return icm::fail(ICM_ERR_ARG, "icm_set_harvest: negative argument");
+    ICM_CUDA(cudaSetDevice(c->device));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    dfree(c->d_harvest);
+    c->harvest_cap = 0;
+    c->harvest_every = 0;
+    if (capacity == 0 || every == 0) return ICM_OK;
+    int rc;
+    if ((rc = dalloc(&c->d_harvest, 6 * (size_t)capacity))) return rc;
+    if (!c->d_harvest_n && (rc = dalloc(&c->d_harvest_n, 1))) return rc;
+    ICM_CUDA(cudaMemset(c->d_harvest_n, 0, sizeof(unsigned)));
+    c->harvest_cap = (unsigned)capacity;
+    c->harvest_every = every;
+    return ICM_OK;
+}
+
+extern "C" int icm_harvest_pairs(icm_ctx *c, const icy_SimParams *p, float *x_out, float *y_out, int cap, int *n_out)
+{
+    if (!c || !p || !x_out || !y_out || !n_out || cap < 0)
+        return icm::fail(ICM_ERR_ARG, "icm_harvest_pairs: bad argument");
+    *n_out = 0;
+    if (!c->d_harvest) return ICM_OK;
+    ICM_CUDA(cudaSetDevice(c->device));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    unsigned got = 0;
+    ICM_CUDA(cudaMemcpy(&got, c->d_harvest_n, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    const int n = (int)std::min<unsigned>(std::min(got, c->harvest_cap), (unsigned)cap);
+    if (n > 0) {
+        float *dx = nullptr, *dy = nullptr;
+        int rc;
+        if ((rc = dalloc(&dx, (size_t)n * 6)) || (rc = dalloc(&dy, (size_t)n * 3))) {
+            dfree(dx);
+            return rc;
+        }
+        const icy_SimParams P = kernel_params(c, p);
+        rc = mlp_label(P, c->d_harvest, n, dx, dy, c->stream);
+        if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess)
+            rc = icm::fail(ICM_ERR_CUDA, "icm_harvest_pairs: labelling");
+        if (!rc && (cudaMemcpy(x_out, dx, sizeof(float) * 6 * n, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                    cudaMemcpy(y_out, dy, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost) != cudaSuccess))
+            rc = icm::fail(ICM_ERR_CUDA, "icm_harvest_pairs: copy");
+        dfree(dx);
+        dfree(dy);
+        if (rc) return rc;
+    }
+    ICM_CUDA(cudaMemset(c->d_harvest_n, 0, sizeof(unsigned)));
+    *n_out = n;
+    return ICM_OK;
+}
 
 extern "C" int icm_host_alloc(void **ptr, size_t bytes)
 {

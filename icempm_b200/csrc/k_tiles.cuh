@@ -46,6 +46,7 @@
 #include <cstdint>
 #include <cuda_pipeline.h>
 #include "mpm_math32.cuh"
+#include "mlp.cuh"
 
 namespace icm {
 
@@ -106,6 +107,7 @@ template <class T> struct Tau { T t00, t01, t10, t11; };
 // FP64 reference form: absolute positions, Fe, Jp_inv in double; meta is
 // the grain id (bits 0-15) and the crushed flag (bits 16-23).
 struct Pol64 {
+    static constexpr bool kSurrogate = false;
     // Bp from raw node velocities, operation order of the reference
     static constexpr bool kRelativeGradient = false;
     using real = double;
@@ -212,6 +214,7 @@ struct Pol64 {
 // FP32 strain form: position = int16 cell + FP32 fraction, H = Fe - I; meta
 // holds the grain's residues and the crushed flag (grain_meta32).
 struct Pol32 {
+    static constexpr bool kSurrogate = false;
     // Bp = 4/h sum W (v_i - v_c) dpos^T with v_c the stencil's centre node:
     // equal to the reference's sum since sum W dpos = 0, but free of the
     // cancellation of a large common velocity (whose FP32 residual would
@@ -346,9 +349,8 @@ struct Pol32 {
         Tau32 t = tau32(invariants32(s.H, k.mu, k.kappa));
         return {t.t00, t.t01, t.t01, t.t11};
     }
-    static __device__ __forceinline__ Tau<float> advance(const icy_SimParams &P, const Consts &k, const Tables &T,
-                                                         St &s, float v0, float v1, const float B[4], float &p_tr,
-                                                         float &q_tr, int &redo)
+    // position and H of the particle after a substep
+    static __device__ __forceinline__ void advect(const Consts &k, St &s, float v0, float v1, const float B[4])
     {
         // position: fraction inside the cell, renormalised to [0, 1)
         float fx = s.fx + v0 * k.dt_h_inv, fy = s.fy + v1 * k.dt_h_inv;
@@ -365,9 +367,30 @@ struct Pol32 {
         s.H.a01 = H.a01 + (c01 + (c00 * H.a01 + c01 * H.a11));
         s.H.a10 = H.a10 + (c10 + (c10 * H.a00 + c11 * H.a10));
         s.H.a11 = H.a11 + (c11 + (c10 * H.a01 + c11 * H.a11));
+    }
+    // the trial state of a crushed particle, for the surrogate's training set
+    static __device__ __forceinline__ void harvest(const Consts &k, const St &s)
+    {
+        if (!k.harvest || !meta32_crushed(s.meta)) return;
+        const unsigned slot = atomicAdd(k.harvest_n, 1u);
+        if (slot >= k.harvest_cap) return;
+        float *h = k.harvest + 6 * (size_t)slot;
+        h[0] = s.H.a00;
+        h[1] = s.H.a01;
+        h[2] = s.H.a10;
+        h[3] = s.H.a11;
+        h[4] = s.Jp;
+        h[5] = __uint_as_float(s.meta);
+    }
+    static __device__ __forceinline__ Tau<float> advance(const icy_SimParams &P, const Consts &k, const Tables &T,
+                                                         St &s, float v0, float v1, const float B[4], float &p_tr,
+                                                         float &q_tr, int &redo)
+    {
+        advect(k, s, v0, v1, B);
         redo = 0;
         Tau32 t;
         if (constitutive32(k, T, s.H, s.meta, p_tr, q_tr, t) == kC32_NEEDS_FP64) {
+            harvest(k, s);
             constitutive32_via64(P, s.H, s.Jp, s.meta, p_tr, q_tr);
             redo = 1;
             return stress(P, k, s);
@@ -386,6 +409,127 @@ struct Pol32 {
     static __device__ __forceinline__ float h(const icy_SimParams &, const Consts &k) { return k.h; }
     static __device__ __forceinline__ float four_h_inv(const icy_SimParams &, const Consts &k) { return k.four_h_inv; }
     static __device__ __forceinline__ float stress_c(const icy_SimParams &, const Consts &k) { return k.stress_c; }
+};
+
+// out-of-line steps of the surrogate form (a crushed particle is rare; the
+// hot loop keeps only the deferred state)
+struct SurrogateOut { M2f H; float Jp, p_tr, q_tr; int accepted; };
+
+// FP64 decomposition of a crushed particle's trial state and the
+// network's input row (normalised features) of this lane
+static __device__ __noinline__ Svd64 surrogate_defer(const icy_SimParams &P, const Consts32 &k,
+                                                     __nv_bfloat16 *row, M2f H, float Jp)
+{
+    const M2d F = {1.0 + (double)H.a00, (double)H.a01, (double)H.a10, 1.0 + (double)H.a11};
+    const Svd64 d = svd2x2_64(F);
+    float x[kMlpIn];
+    mlp_features(P, d.s0, d.s1, (double)Jp, x);
+#pragma unroll
+    for (int j = 0; j < 16; j++) row[j] = __float2bfloat16(j < kMlpIn ? (x[j] - k.mlp->x_mu[j]) * k.mlp->x_isd[j] : 0.f);
+    return d;
+}
+
+// applies the network's output y (normalised) when it meets the yield
+// condition it stands for, else the exact projection
+static __device__ __noinline__ SurrogateOut surrogate_finish(const icy_SimParams &P, const Consts32 &k, const float *y,
+                                                             M2f H, float Jp, Svd64 d)
+{
+    const double s0 = d.s0, s1 = d.s1, jp = Jp;
+    // p and q of the trial state (ComputePQ, gpu_implementation5.cu:36-44)
+    const double Je = s0 * s1, ptr = -(P.kappa / 2.) * (Je * Je - 1.);
+    const double sq0 = s0 * s0, sq1 = s1 * s1, qtr = P.mu / Je * fabs(sq0 - sq1);
+    const double s0n = s0 + 1e-3 * (double)(y[0] * k.mlp->y_sd[0] + k.mlp->y_mu[0]);
+    const double s1n = s1 + 1e-3 * (double)(y[1] * k.mlp->y_sd[1] + k.mlp->y_mu[1]);
+    const double tol = k.mlp_tol, p_thr = P.DP_threshold_p;
+    DpResult r{false, s0, s1, jp};
+    bool ok = false;
+    if (!(ptr < -p_thr || jp < 1) && isfinite(s0n) && isfinite(s1n) && s0n > 0 && s1n > 0) {
+        const double q_n_1 =
+            (ptr > P.IceCompressiveStrength) ? 0.0 : fmin((ptr + p_thr) * P.DP_tan_phi, P.IceShearStrength);
+        if (qtr >= q_n_1) {
+            const double sq0n = s0n * s0n, sq1n = s1n * s1n, qn = P.mu / (s0n * s1n) * fabs(sq0n - sq1n);
+            ok = fabs(qn - q_n_1) <= tol * P.IceShearStrength && fabs((sq0n + sq1n) - (sq0 + sq1)) <= tol * 1e-3;
+            r = {true, s0n, s1n, jp};
+        } else {
+            ok = fabs(s0n - s0) <= tol * 1e-3 && fabs(s1n - s1) <= tol * 1e-3;
+        }
+    }
+    if (!ok) r = dp_project64(P, s0, s1, jp);
+    SurrogateOut o{H, Jp, (float)ptr, (float)qtr, ok ? 1 : 0};
+    if (r.changed) {
+        const M2d Fe = usvt64(d, r.s0, r.s1);
+        o.H = {(float)(Fe.a00 - 1.0), (float)Fe.a01, (float)Fe.a10, (float)(Fe.a11 - 1.0)};
+        o.Jp = (float)r.jp;
+    }
+    return o;
+}
+
+// FP32 strain form with the learned Drucker-Prager projection (mlp.cuh).
+// A crushed particle is decomposed in FP64 as in the FP32 form; instead of
+// the exact projection (dp_project64) the network predicts the new
+// singular values, once per round for the whole warp (advance defers the
+// particle, network runs the warp, finish applies the result). The
+// prediction is accepted when it satisfies the yield condition it stands
+// for within mlp_tol: on the surface q = q_n+1 with the trial mean of
+// sigma^2 kept (pressure kept), or unchanged when the trial state lies
+// inside; otherwise, and for the hydrostatic branch (p < -p_thr or
+// Jp_inv < 1, a closed form with nothing to learn), the exact map runs.
+struct Pol32S : Pol32 {
+    static constexpr bool kSurrogate = true;
+    struct Tables : GrainTables32 {
+        __nv_bfloat16 xrow[kMaxWarps][32 * 16];  // normalised network inputs, one row per lane
+        float yrow[kMaxWarps][32 * 4];           // normalised outputs
+    };
+    struct St : Pol32::St { Svd64 d; };
+    static __device__ __forceinline__ St load_staged(const Stage &S, int lane)
+    {
+        St s;
+        static_cast<Pol32::St &>(s) = Pol32::load_staged(S, lane);
+        return s;
+    }
+    static __device__ __forceinline__ Tau<float> advance(const icy_SimParams &P, const Consts &k, Tables &T, St &s,
+                                                         float v0, float v1, const float B[4], float &p_tr,
+                                                         float &q_tr, int &redo)
+    {
+        advect(k, s, v0, v1, B);
+        redo = 0;
+        Tau32 t;
+        if (constitutive32(k, T, s.H, s.meta, p_tr, q_tr, t) == kC32_OK) return {t.t00, t.t01, t.t01, t.t11};
+        harvest(k, s);
+        if (k.mlp && meta32_crushed(s.meta)) {
+            s.d = surrogate_defer(P, k, T.xrow[threadIdx.x >> 5] + (threadIdx.x & 31) * 16, s.H, s.Jp);
+            redo = 2;
+            return {0.f, 0.f, 0.f, 0.f};
+        }
+        constitutive32_via64(P, s.H, s.Jp, s.meta, p_tr, q_tr);
+        redo = 1;
+        return stress(P, k, s);
+    }
+    // warp-collective: lanes without a deferred particle feed zeros
+    static __device__ __forceinline__ void network(const Consts &k, Tables &T, bool mine)
+    {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (!mine) {
+            uint32_t *row = reinterpret_cast<uint32_t *>(T.xrow[warp] + lane * 16);
+#pragma unroll
+            for (int j = 0; j < 8; j++) row[j] = 0u;
+        }
+        warp_mlp(k.mlp, T.xrow[warp], T.yrow[warp]);
+    }
+    static __device__ __forceinline__ Tau<float> finish(const icy_SimParams &P, const Consts &k, const Tables &T,
+                                                        St &s, float &p_tr, float &q_tr, unsigned &accepted,
+                                                        unsigned &exact)
+    {
+        const SurrogateOut o =
+            surrogate_finish(P, k, T.yrow[threadIdx.x >> 5] + (threadIdx.x & 31) * 4, s.H, s.Jp, s.d);
+        s.H = o.H;
+        s.Jp = o.Jp;
+        p_tr = o.p_tr;
+        q_tr = o.q_tr;
+        accepted += o.accepted;
+        exact += 1 - o.accepted;
+        return stress(P, k, s);
+    }
 };
 
 // ------------------------------------------------------- grid node access
@@ -605,7 +749,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     constexpr int CELLS = TX * TY;
     constexpr int NGT = CELLS / 32;  // groups of 32 cells in the tile
     int bad = 0;
-    unsigned redo_count = 0, stray_count = 0;
+    unsigned redo_count = 0, stray_count = 0, mlp_ok = 0, mlp_fb = 0;
     Acc *wacc = s_acc + warp * RN;
     typename Pol::Stage *stage =
         reinterpret_cast<typename Pol::Stage *>(s_dyn + tile_region_bytes<Pol, MODE>(RN, nwarps)) + 2 * warp;
@@ -659,6 +803,87 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
 #pragma unroll
             for (int q = 0; q < 9; q++) { am[q] = 0; ax[q] = 0; ay[q] = 0; }
         }
+        // P2G of one (updated) particle: node (i, j) gets
+        // W_ij (m, c + S_h (i, j)^T) with S = m Bp - dt Vp Dinv tau
+        auto p2g = [&](const typename Pol::St &s, const real v0, const real v1, const real *B,
+                       const Tau<real> &tau) {
+            const typename Pol::Sten st = Pol::stencil(P, K, s);
+            const real S00 = h * (m * B[0] - sc * tau.t00), S01 = h * (m * B[1] - sc * tau.t01);
+            const real S10 = h * (m * B[2] - sc * tau.t10), S11 = h * (m * B[3] - sc * tau.t11);
+            const real c0 = v0 * m - (S00 * st.fx + S01 * st.fy);
+            const real c1 = v1 * m - (S10 * st.fx + S11 * st.fy);
+            if (cell_ok && st.bx == cbx && st.by == cby) {
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
+                    const real wm = st.wx[i] * m;
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        const real W = st.wx[i] * st.wy[j];
+                        am[i * 3 + j] += wm * st.wy[j];
+                        ax[i * 3 + j] += W * (u0 + S01 * (real)j);
+                        ay[i * 3 + j] += W * (u1 + S11 * (real)j);
+                    }
+                }
+            } else {
+                stray_count++;
+                const int lx = st.bx - rx0, ly = st.by - ry0;
+                const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 &&
+                                    st.by >= 0 && st.bx + 2 < GX && st.by + 2 < GY;
+#pragma unroll 1
+                for (int i = 0; i < 3; i++) {
+                    real cm[3], cx[3], cy[3];
+                    const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        const real W = st.wx[i] * st.wy[j];
+                        cm[j] = W * m;
+                        cx[j] = W * (u0 + S01 * (real)j);
+                        cy[j] = W * (u1 + S11 * (real)j);
+                    }
+                    if (inside) {
+#pragma unroll
+                        for (int j = 0; j < 3; j++) {
+                            real *ap = reinterpret_cast<real *>(&wacc[(ly + j) * RX + lx + i]);
+                            atomicAdd(ap + 0, cm[j]);
+                            atomicAdd(ap + 1, cx[j]);
+                            atomicAdd(ap + 2, cy[j]);
+                        }
+                    } else {
+                        bad |= far_scatter<Pol, TX, TY>(GX, GY, gB, R.dirty[R.bufB], R.ntx, st.bx + i, st.by,
+                                                        cm[0], cm[1], cm[2], cx[0], cx[1], cx[2], cy[0], cy[1],
+                                                        cy[2]);
+                    }
+                }
+            }
+        };
+        // the lane's cell sums into the warp's region: 9 read-modify-write
+        // steps, one warp barrier after each (two cells a row apart reach
+        // the same node in different steps)
+        auto flush_cell_sums = [&]() {
+            const int ckey = (cly + 1) * RX + (clx + 1);
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    if (cnt > 0 && cell_ok) {
+                        Acc &ac = wacc[ckey + j * RX + i];
+                        Acc v = ac;
+                        acc_add(v, am[i * 3 + j], ax[i * 3 + j], ay[i * 3 + j]);
+                        ac = v;
+                    }
+                    __syncwarp();
+                }
+        };
+        struct Deferred {
+            int p;
+            typename Pol::St s;
+            real v0, v1, B[4];
+            decltype(Pol::St::Jp) jp_old;
+            uint32_t meta_old;
+        } dfr;
+        bool deferred = false;
         if (r < cnt) {
             const int p = s_wgbase[warp][k] + 32 * r + lane;
             typename Pol::St s = Pol::load_staged(stage[cur], lane);
@@ -737,85 +962,49 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                 real p_tr, q_tr;
                 int redo;
                 tau = Pol::advance(P, K, s_tab, s, v0, v1, B, p_tr, q_tr, redo);
-                redo_count += redo;
-                Pol::store(A, p, s, jp_old, meta_old);
-                if (R.record_pq) A.pq[p] = {p_tr, q_tr};
-                if (MODE == kModeFinal) {
-                    A.vel[p] = {v0, v1};
-                    A.Bp[p] = {B[0], B[1], B[2], B[3]};
+                if (Pol::kSurrogate && redo == 2) {
+                    deferred = true;
+                    dfr = {p, s, v0, v1, {B[0], B[1], B[2], B[3]}, jp_old, meta_old};
+                } else {
+                    redo_count += redo;
+                    Pol::store(A, p, s, jp_old, meta_old);
+                    if (R.record_pq) A.pq[p] = {p_tr, q_tr};
+                    if (MODE == kModeFinal) {
+                        A.vel[p] = {v0, v1};
+                        A.Bp[p] = {B[0], B[1], B[2], B[3]};
+                    }
                 }
             }
-            if (do_p2g) {
-                // P2G of the (updated) particle: node (i, j) gets
-                // W_ij (m, c + S_h (i, j)^T) with S = m Bp - dt Vp Dinv tau
-                const typename Pol::Sten st = Pol::stencil(P, K, s);
-                const real S00 = h * (m * B[0] - sc * tau.t00), S01 = h * (m * B[1] - sc * tau.t01);
-                const real S10 = h * (m * B[2] - sc * tau.t10), S11 = h * (m * B[3] - sc * tau.t11);
-                const real c0 = v0 * m - (S00 * st.fx + S01 * st.fy);
-                const real c1 = v1 * m - (S10 * st.fx + S11 * st.fy);
-                if (cell_ok && st.bx == cbx && st.by == cby) {
+            if (do_p2g && !deferred) p2g(s, v0, v1, B, tau);
+        }
+        // surrogate form: particles whose projection the network makes were
+        // held back above; the whole warp now evaluates the network
+        if constexpr (Pol::kSurrogate) {
+            if (__any_sync(FULL, deferred)) {
+                // the sums are additive: hand them to the warp's region now so
+                // that they are not held across the network's call
+                if (MODE != kModeFinal) {
+                    flush_cell_sums();
 #pragma unroll
-                    for (int i = 0; i < 3; i++) {
-                        const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
-                        const real wm = st.wx[i] * m;
-#pragma unroll
-                        for (int j = 0; j < 3; j++) {
-                            const real W = st.wx[i] * st.wy[j];
-                            am[i * 3 + j] += wm * st.wy[j];
-                            ax[i * 3 + j] += W * (u0 + S01 * (real)j);
-                            ay[i * 3 + j] += W * (u1 + S11 * (real)j);
-                        }
+                    for (int q = 0; q < 9; q++) { am[q] = 0; ax[q] = 0; ay[q] = 0; }
+                }
+                Pol::network(K, s_tab, deferred);
+                if (deferred) {
+                    real p_tr, q_tr;
+                    const Tau<real> t2 = Pol::finish(P, K, s_tab, dfr.s, p_tr, q_tr, mlp_ok, mlp_fb);
+                    redo_count += 1;
+                    Pol::store(A, dfr.p, dfr.s, dfr.jp_old, dfr.meta_old);
+                    if (R.record_pq) A.pq[dfr.p] = {p_tr, q_tr};
+                    if (MODE == kModeFinal) {
+                        A.vel[dfr.p] = {dfr.v0, dfr.v1};
+                        A.Bp[dfr.p] = {dfr.B[0], dfr.B[1], dfr.B[2], dfr.B[3]};
                     }
-                } else {
-                    stray_count++;
-                    const int lx = st.bx - rx0, ly = st.by - ry0;
-                    const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 &&
-                                        st.by >= 0 && st.bx + 2 < GX && st.by + 2 < GY;
-#pragma unroll 1
-                    for (int i = 0; i < 3; i++) {
-                        real cm[3], cx[3], cy[3];
-                        const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
-#pragma unroll
-                        for (int j = 0; j < 3; j++) {
-                            const real W = st.wx[i] * st.wy[j];
-                            cm[j] = W * m;
-                            cx[j] = W * (u0 + S01 * (real)j);
-                            cy[j] = W * (u1 + S11 * (real)j);
-                        }
-                        if (inside) {
-#pragma unroll
-                            for (int j = 0; j < 3; j++) {
-                                real *ap = reinterpret_cast<real *>(&wacc[(ly + j) * RX + lx + i]);
-                                atomicAdd(ap + 0, cm[j]);
-                                atomicAdd(ap + 1, cx[j]);
-                                atomicAdd(ap + 2, cy[j]);
-                            }
-                        } else {
-                            bad |= far_scatter<Pol, TX, TY>(GX, GY, gB, R.dirty[R.bufB], R.ntx, st.bx + i, st.by,
-                                                            cm[0], cm[1], cm[2], cx[0], cx[1], cx[2], cy[0], cy[1],
-                                                            cy[2]);
-                        }
-                    }
+                    if (MODE != kModeFinal) p2g(dfr.s, dfr.v0, dfr.v1, dfr.B, t2);
                 }
             }
         }
         // last round of this group: its cells' sums go to the warp's region
-        if (MODE != kModeFinal && nk != k) {
-            const int ckey = (cly + 1) * RX + (clx + 1);
-            __syncwarp();
-#pragma unroll
-            for (int i = 0; i < 3; i++)
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    if (cnt > 0 && cell_ok) {
-                        Acc &ac = wacc[ckey + j * RX + i];
-                        Acc v = ac;
-                        acc_add(v, am[i * 3 + j], ax[i * 3 + j], ay[i * 3 + j]);
-                        ac = v;
-                    }
-                    __syncwarp();
-                }
-        }
+        if (MODE != kModeFinal && nk != k) flush_cell_sums();
         k = nk;
         r = nr;
         cur ^= 1;
@@ -824,6 +1013,10 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     if (stray_count && R.strays) atomicAdd(R.strays, (unsigned long long)stray_count);
     if (bad) *R.err = 1;
     if (redo_count && R.fp64_redo) atomicAdd(R.fp64_redo, (unsigned long long)redo_count);
+    if constexpr (Pol::kSurrogate) {
+        if (mlp_ok) atomicAdd(&K.mlp_counts[0], (unsigned long long)mlp_ok);
+        if (mlp_fb) atomicAdd(&K.mlp_counts[1], (unsigned long long)mlp_fb);
+    }
     if (MODE == kModeFinal) return;
     __syncthreads();
 

@@ -32,6 +32,7 @@
 namespace icm {
 
 struct M2f { float a00, a01, a10, a11; };
+struct MlpWarpNet;
 
 // Per-run FP32 constants, derived on the host in double.
 struct Consts32 {
@@ -40,6 +41,15 @@ struct Consts32 {
     float gv, ics, its, iss;                        // grain variability, strengths in MPa
     float four_h_inv;
     float dt_g, vmax;                               // dt*gravity, 0.5 h/dt
+    // trial states of crushed particles (H, Jp_inv, meta: 6 words each) are
+    // appended here while harvest is set (training data of the surrogate)
+    float *harvest;
+    unsigned *harvest_n;
+    unsigned harvest_cap;
+    // surrogate form: network, acceptance tolerance, counters {accepted, exact}
+    const MlpWarpNet *mlp;
+    float mlp_tol;
+    unsigned long long *mlp_counts;
 };
 
 // Grain strengths in MPa by residue (gpu_implementation5.cu:97-105): the

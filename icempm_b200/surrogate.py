@@ -40,6 +40,10 @@ def _sigs():
         ("icm_mlp_train", i, [i, vp, vp, i, C.POINTER(TrainCfg), vp, vp]),
         ("icm_mlp_gradient", i, [i, vp, vp, vp, i, vp, vp]),
         ("icm_mlp_infer", i, [i, vp, vp, i, vp, i]),
+        ("icm_set_surrogate", i, [vp, vp, f]),
+        ("icm_surrogate_counts", i, [vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
+        ("icm_set_harvest", i, [vp, i, i]),
+        ("icm_harvest_pairs", i, [vp, vp, vp, vp, i, C.POINTER(i)]),
     ):
         fn = getattr(L, name)
         fn.restype = res
@@ -115,3 +119,49 @@ def infer(net: np.ndarray, x: np.ndarray, warp_form: bool = False, device: int =
     _check(_sigs().icm_mlp_infer(device, net.ctypes.data, x.ctypes.data, len(x), y.ctypes.data,
                                  1 if warp_form else 0))
     return y
+
+
+# ------------------------------------------------- the surrogate form
+
+def set_surrogate(gpu, net, tolerance: float = 0.02) -> None:
+    """Gives a GPU_Implementation5 the network of its surrogate form
+    (FORM_FP32_SURROGATE); None removes it."""
+    gpu.initialize()
+    if net is None:
+        _check(_sigs().icm_set_surrogate(gpu._ctx, None, C.c_float(0)))
+        return
+    net = _f32(net)
+    _check(_sigs().icm_set_surrogate(gpu._ctx, net.ctypes.data, C.c_float(tolerance)))
+
+
+def counts(gpu):
+    """(network projections accepted, exact projections) since set_surrogate."""
+    a, e = C.c_ulonglong(0), C.c_ulonglong(0)
+    _check(_sigs().icm_surrogate_counts(gpu._ctx, C.byref(a), C.byref(e)))
+    return int(a.value), int(e.value)
+
+
+def set_harvest(gpu, capacity: int, every: int = 1) -> None:
+    """Record crushed particles' trial states on every `every`-th substep
+    of the fused FP32 forms (capacity 0: off)."""
+    gpu.initialize()
+    _check(_sigs().icm_set_harvest(gpu._ctx, capacity, every))
+
+
+def harvest_pairs(gpu, prms, cap: int):
+    """The recorded states labelled by the exact projection: (x n x 6, y n x 3)."""
+    x = np.zeros((cap, N_IN), dtype=np.float32)
+    y = np.zeros((cap, N_OUT), dtype=np.float32)
+    n = C.c_int(0)
+    _check(_sigs().icm_harvest_pairs(gpu._ctx, C.byref(prms), x.ctypes.data, y.ctypes.data, cap, C.byref(n)))
+    return x[: n.value], y[: n.value]
+
+
+def fit(x: np.ndarray, y: np.ndarray, steps: int = 3000, batch_tiles: int = 32, lr: float = 3e-3, seed: int = 0,
+        device: int = 0):
+    """A network trained on labelled pairs: normalisation from the data,
+    seeded initial weights, Adam on the tensor cores. Returns (net, loss)."""
+    net = init_net(seed)
+    normalise(net, x, y)
+    loss = train(net, x, y, steps=steps, batch_tiles=batch_tiles, lr=lr, seed=seed + 1, device=device)
+    return net, loss

@@ -45,7 +45,8 @@ enum {
 enum {
     ICM_FORM_FP64_STEPWISE = 0, /* reference structure: reset, P2G, update, G2P launches per substep, FP64 */
     ICM_FORM_FP64 = 1,          /* fused tile substep, FP64 reference form */
-    ICM_FORM_FP32 = 2           /* fused tile substep, FP32 strain form */
+    ICM_FORM_FP32 = 2,          /* fused tile substep, FP32 strain form */
+    ICM_FORM_FP32_SURROGATE = 3 /* FP32 form with the learned Drucker-Prager projection (icm_set_surrogate) */
 };
 
 typedef struct icm_ctx icm_ctx;
@@ -228,6 +229,24 @@ int icm_mlp_gradient(int device, const float *net, const float *x, const float *
 /* Network outputs (denormalised, n x 3) for n inputs: the tensor-core
  * batch form (warp_form = 0) or the warp form the substep uses (1). */
 int icm_mlp_infer(int device, const float *net, const float *x, int n, float *y, int warp_form);
+/* The surrogate form's network (NULL: none) and acceptance tolerance tau:
+ * the network's projection of a crushed particle is used when it meets the
+ * yield condition to within tau * IceShearStrength in q and tau * 1e-3 in
+ * the stretches (the sum of squared stretches, i.e. the pressure, kept);
+ * otherwise the exact projection runs. Resets the counters. */
+int icm_set_surrogate(icm_ctx *ctx, const float *net, float tolerance);
+/* Crushed-particle updates of the surrogate form since the network was
+ * set: network projections accepted, and exact projections (rejected
+ * predictions plus the hydrostatic branch, a closed form). */
+int icm_surrogate_counts(icm_ctx *ctx, unsigned long long *accepted, unsigned long long *exact);
+/* Training data: the fused FP32 forms record the trial state of every
+ * crushed particle on substeps with (SimulationStep % every == 0), up to
+ * capacity states (capacity or every 0: off). */
+int icm_set_harvest(icm_ctx *ctx, int capacity, int every);
+/* Labels the recorded states with the exact projection on the GPU and
+ * returns up to cap pairs (features n x 6, targets n x 3); clears the
+ * record. */
+int icm_harvest_pairs(icm_ctx *ctx, const icy_SimParams *p, float *x, float *y, int cap, int *n_out);
 
 /* ------------------------------------------------------------ snapshots
  * SnapshotManager (simulation/snapshotmanager.cpp) on the library's own
