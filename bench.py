@@ -34,6 +34,10 @@ METRIC = "particle-updates/s at 1M pts: FP32/learned vs plain FP64, 1 B200, ≤1
 UNIT = "particle-updates/s"
 L2_FLUSH_BYTES = 256 << 20
 SENS_NOISE = 3e-8  # std of the initial Fe perturbation of the FP64 sensitivity run
+LATE_SUBSTEPS = 200  # launches timed after a full frame (crushed particles present)
+# learned projection: pairs harvested from the 250k-particle workload
+HARVEST_CONFIG, HARVEST_EVERY, HARVEST_CAP = "c2_250k", 5, 4_000_000
+SUR_STEPS, SUR_TILES, SUR_TOL = 3000, 64, 0.02
 
 
 def parse():
@@ -50,6 +54,7 @@ def parse():
     a.add_argument("--no-accuracy", action="store_true")
     a.add_argument("--no-cpu", action="store_true")
     a.add_argument("--no-fp64", action="store_true")
+    a.add_argument("--no-surrogate", action="store_true")
     a.add_argument("--form", choices=["fp32", "fp64"], default="fp32",
                    help="fused form of the headline (fp64: for profiling the FP64 fused kernel)")
     return a.parse_args()
@@ -375,6 +380,17 @@ def main():
         nsub = configs.CONFIGS[name][6]
         res = {}
         strays = {}
+        late = {}
+
+        def late_launch_us(mm):
+            """Average fused launch after the frame: the crushed zone at the
+            indenter is then fully developed."""
+            mm.gpu.kernel_timing(True)
+            mm.gpu.run_substeps(mm.prms, LATE_SUBSTEPS)
+            kms2, kn2 = mm.gpu.kernel_time()
+            mm.gpu.kernel_timing(False)
+            return 1e3 * kms2 / max(kn2, 1)
+
         for form in (im.FORM_FP64, im.FORM_FP32, im.FORM_FP64_STEPWISE):
             mm = make(form, tile64 if form != im.FORM_FP32 else tile, threads64 if form != im.FORM_FP32 else None)
             mm.gpu.run_substeps(mm.prms, nsub)
@@ -384,6 +400,8 @@ def main():
             mm.gpu.cuda_transfer_from_device()
             mm.gpu.synchronize()
             res[form] = (hist, mm.gpu.tmp_transfer_buffer.copy(), mm.gpu.error_code)
+            if form != im.FORM_FP64_STEPWISE:
+                late[im.FORM_NAMES[form]] = late_launch_us(mm)
             mm.gpu.close()
         h64, s64, e64 = res[im.FORM_FP64]
         h32, s32, e32 = res[im.FORM_FP32]
@@ -437,9 +455,69 @@ def main():
                                                             x64).max(axis=0), 99) / p0.cellsize),
             },
             "error_flags": [int(e64), int(e32), int(esw)],
+            "late_frame_us_per_launch": late,
             "fp64_fallback_particles": redo,
             "stray_particle_substeps": {"fp64": strays.get(im.FORM_FP64), "fp32": strays.get(im.FORM_FP32)},
         }
+
+        # --- the learned projection: pairs harvested from the FP32 form on the
+        # 250k-particle workload, trained on the tensor cores, then the
+        # surrogate form on this workload
+        if not args.no_surrogate:
+            from icempm_b200 import surrogate as sg
+
+            t0 = time.perf_counter()
+            mh = configs.load_model(HARVEST_CONFIG, local)
+            mh.gpu.set_form(im.FORM_FP32)
+            mh.gpu.set_tile(1, 128)
+            sg.set_harvest(mh.gpu, HARVEST_CAP, HARVEST_EVERY)
+            mh.gpu.run_substeps(mh.prms, configs.CONFIGS[HARVEST_CONFIG][6])
+            xh, yh = sg.harvest_pairs(mh.gpu, mh.prms, HARVEST_CAP)
+            mh.gpu.close()
+            t1 = time.perf_counter()
+            net, loss = sg.fit(xh, yh, steps=SUR_STEPS, batch_tiles=SUR_TILES, lr=3e-3, seed=0, device=local)
+            t2 = time.perf_counter()
+            # throughput at the start of the frame, as the headline
+            mt = make(im.FORM_FP32_SURROGATE, tile, 128)
+            sg.set_surrogate(mt.gpu, net, SUR_TOL)
+            k2 = max(2, args.steps // 3)
+            ms3, (k3ms, k3n) = timed(mt, k2, 1, args.substeps, ktime=True)
+            mt.gpu.close()
+            # accuracy over the full frame, and the late-frame launch
+            ms_ = make(im.FORM_FP32_SURROGATE, tile, 128)
+            sg.set_surrogate(ms_.gpu, net, SUR_TOL)
+            ms_.gpu.run_substeps(ms_.prms, nsub)
+            hs = ms_.gpu.force_history(nsub)
+            ms_.gpu.cuda_transfer_from_device()
+            ms_.gpu.synchronize()
+            ss = ms_.gpu.tmp_transfer_buffer.copy()
+            acc_n, exact_n = sg.counts(ms_.gpu)
+            late_s = late_launch_us(ms_)
+            ms_.gpu.close()
+            fs = np.hypot(hs[:, 0], hs[:, 1])
+            xs = ss[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n]
+            v3 = n * args.substeps * k2 / (sum(ms3) / 1e3)
+            a3 = alg_bytes("fp32", n, na, ng) / (k3ms / max(k3n, 1) / 1e3) / 1e9
+            extra["surrogate"] = {
+                "value": v3, "unit": UNIT, "ms_per_step": sum(ms3) / k2, "steps": k2,
+                "speedup_vs_fp64_stepwise": (v3 / extra["fp64_stepwise"]["value"]) if "fp64_stepwise" in extra else None,
+                "roofline": {"achieved": a3, "frac": a3 / hbm, "avg_launch_us": 1e3 * k3ms / max(k3n, 1)},
+                "late_frame_us_per_launch": late_s,
+                "training": {"pairs": int(len(xh)), "harvested_from": f"{HARVEST_CONFIG}, FP32 form, every "
+                                                                       f"{HARVEST_EVERY} substeps of a 10,000-substep frame",
+                             "steps": SUR_STEPS, "batch": 128 * SUR_TILES, "first_loss": float(loss[:10].mean()),
+                             "final_loss": float(loss[-100:].mean()), "harvest_s": t1 - t0, "train_s": t2 - t1},
+                "tolerance": SUR_TOL,
+                "network_projections_accepted": acc_n, "exact_projections": exact_n,
+                "accuracy_vs_fp64": {
+                    "peak_force_rel_err": float(abs(fs.max() - f64.max()) / max(f64.max(), 1e-30)),
+                    "peak_force_rel_err_100substep_avg": float(abs(smooth(fs).max() - smooth(f64).max()) /
+                                                               max(smooth(f64).max(), 1e-30)),
+                    "frame_impulse_rel_err": float(abs(fs.sum() - f64.sum()) / max(abs(f64.sum()), 1e-30)),
+                    "max_pos_err_h": float(np.abs(xs - x64).max() / p0.cellsize),
+                    "p99_pos_err_h": float(np.percentile(np.abs(xs - x64).max(axis=0), 99) / p0.cellsize),
+                },
+            }
 
     # --- end to end: one frame through the public API with host buffers
     e2e = None

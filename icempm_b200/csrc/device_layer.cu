@@ -593,6 +593,8 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     icy_SimParams P = kernel_params(c, p);
     if (c->form == ICM_FORM_FP32_SURROGATE && !c->d_mlp)
         return icm::fail(ICM_ERR_STATE, "surrogate form without a network (icm_set_surrogate)");
+    if (c->form == ICM_FORM_FP32_SURROGATE && c->threads > 32 * Pol32S::kWarps)
+        return icm::fail(ICM_ERR_ARG, "surrogate form: at most 128 threads per block");
     if (!c->internal_valid || c->fz.form != storage_form(c->form) || c->internal_variant != c->tile_variant) {
         int rc = ensure_ref(c);
         if (rc) return rc;

@@ -108,6 +108,7 @@ template <class T> struct Tau { T t00, t01, t10, t11; };
 // the grain id (bits 0-15) and the crushed flag (bits 16-23).
 struct Pol64 {
     static constexpr bool kSurrogate = false;
+    static constexpr int kMinBlocks = 0;
     // Bp from raw node velocities, operation order of the reference
     static constexpr bool kRelativeGradient = false;
     using real = double;
@@ -215,6 +216,7 @@ struct Pol64 {
 // holds the grain's residues and the crushed flag (grain_meta32).
 struct Pol32 {
     static constexpr bool kSurrogate = false;
+    static constexpr int kMinBlocks = 0;  // no residency hint: the compiler's own register choice
     // Bp = 4/h sum W (v_i - v_c) dpos^T with v_c the stencil's centre node:
     // equal to the reference's sum since sum W dpos = 0, but free of the
     // cancellation of a large common velocity (whose FP32 residual would
@@ -415,25 +417,27 @@ struct Pol32 {
 // hot loop keeps only the deferred state)
 struct SurrogateOut { M2f H; float Jp, p_tr, q_tr; int accepted; };
 
-// FP64 decomposition of a crushed particle's trial state and the
-// network's input row (normalised features) of this lane
-static __device__ __noinline__ Svd64 surrogate_defer(const icy_SimParams &P, const Consts32 &k,
-                                                     __nv_bfloat16 *row, M2f H, float Jp)
+// the network's input row (normalised features) of a crushed particle
+// from the FP64 decomposition of its trial state
+static __device__ __noinline__ void surrogate_defer(const icy_SimParams &P, const Consts32 &k, __nv_bfloat16 *row,
+                                                   M2f H, float Jp)
 {
     const M2d F = {1.0 + (double)H.a00, (double)H.a01, (double)H.a10, 1.0 + (double)H.a11};
     const Svd64 d = svd2x2_64(F);
     float x[kMlpIn];
     mlp_features(P, d.s0, d.s1, (double)Jp, x);
 #pragma unroll
-    for (int j = 0; j < 16; j++) row[j] = __float2bfloat16(j < kMlpIn ? (x[j] - k.mlp->x_mu[j]) * k.mlp->x_isd[j] : 0.f);
-    return d;
+    for (int j = 0; j < 8; j++) row[j] = __float2bfloat16(j < kMlpIn ? (x[j] - k.mlp->x_mu[j]) * k.mlp->x_isd[j] : 0.f);
 }
 
 // applies the network's output y (normalised) when it meets the yield
-// condition it stands for, else the exact projection
+// condition it stands for, else the exact projection; the decomposition is
+// redone here rather than carried through the round in registers
 static __device__ __noinline__ SurrogateOut surrogate_finish(const icy_SimParams &P, const Consts32 &k, const float *y,
-                                                             M2f H, float Jp, Svd64 d)
+                                                             M2f H, float Jp)
 {
+    const M2d F = {1.0 + (double)H.a00, (double)H.a01, (double)H.a10, 1.0 + (double)H.a11};
+    const Svd64 d = svd2x2_64(F);
     const double s0 = d.s0, s1 = d.s1, jp = Jp;
     // p and q of the trial state (ComputePQ, gpu_implementation5.cu:36-44)
     const double Je = s0 * s1, ptr = -(P.kappa / 2.) * (Je * Je - 1.);
@@ -476,16 +480,44 @@ static __device__ __noinline__ SurrogateOut surrogate_finish(const icy_SimParams
 // Jp_inv < 1, a closed form with nothing to learn), the exact map runs.
 struct Pol32S : Pol32 {
     static constexpr bool kSurrogate = true;
+    static constexpr int kMinBlocks = 0;
+    // at most kWarps warps per CTA (128 threads) in this form
+    static constexpr int kWarps = 4;
+    // A particle held back for the network: slot, state after advection,
+    // velocity and gradient for its P2G (its Jp_inv and meta word are still
+    // the stored ones and are read back from the particle arrays). Kept in
+    // shared memory, not registers, so the round's register use is the FP32
+    // form's; with the network's rows the extra is 9 KB per CTA, which
+    // keeps four 128-thread CTAs per SM.
+    struct Held { int p; uint32_t cell; float fx, fy, H[4], v0, v1, B[4]; };
     struct Tables : GrainTables32 {
-        __nv_bfloat16 xrow[kMaxWarps][32 * 16];  // normalised network inputs, one row per lane
-        float yrow[kMaxWarps][32 * 4];           // normalised outputs
+        alignas(16) unsigned char rows[kWarps][32 * 16];  // network input/output rows, one per lane
+        Held held[kWarps][32];
     };
-    struct St : Pol32::St { Svd64 d; };
-    static __device__ __forceinline__ St load_staged(const Stage &S, int lane)
+    static __device__ __forceinline__ void defer_save(Tables &T, int p, const St &s, float v0, float v1,
+                                                      const float B[4], float, uint32_t)
     {
-        St s;
-        static_cast<Pol32::St &>(s) = Pol32::load_staged(S, lane);
-        return s;
+        T.held[threadIdx.x >> 5][threadIdx.x & 31] = {p, pack_cell(s.ix, s.iy), s.fx, s.fy,
+                                                      {s.H.a00, s.H.a01, s.H.a10, s.H.a11}, v0, v1,
+                                                      {B[0], B[1], B[2], B[3]}};
+    }
+    static __device__ __forceinline__ void defer_load(const Tables &T, const Parts &A, int &p, St &s, float &v0,
+                                                      float &v1, float B[4], float &jp_old, uint32_t &meta_old)
+    {
+        const Held &h = T.held[threadIdx.x >> 5][threadIdx.x & 31];
+        p = h.p;
+        s.ix = cell_x(h.cell);
+        s.iy = cell_y(h.cell);
+        s.fx = h.fx;
+        s.fy = h.fy;
+        s.H = {h.H[0], h.H[1], h.H[2], h.H[3]};
+        s.Jp = A.Jp[p];
+        s.meta = A.meta[p];
+        v0 = h.v0;
+        v1 = h.v1;
+        for (int j = 0; j < 4; j++) B[j] = h.B[j];
+        jp_old = s.Jp;
+        meta_old = s.meta;
     }
     static __device__ __forceinline__ Tau<float> advance(const icy_SimParams &P, const Consts &k, Tables &T, St &s,
                                                          float v0, float v1, const float B[4], float &p_tr,
@@ -497,7 +529,9 @@ struct Pol32S : Pol32 {
         if (constitutive32(k, T, s.H, s.meta, p_tr, q_tr, t) == kC32_OK) return {t.t00, t.t01, t.t01, t.t11};
         harvest(k, s);
         if (k.mlp && meta32_crushed(s.meta)) {
-            s.d = surrogate_defer(P, k, T.xrow[threadIdx.x >> 5] + (threadIdx.x & 31) * 16, s.H, s.Jp);
+            surrogate_defer(P, k,
+                            reinterpret_cast<__nv_bfloat16 *>(T.rows[threadIdx.x >> 5] + (threadIdx.x & 31) * 16),
+                            s.H, s.Jp);
             redo = 2;
             return {0.f, 0.f, 0.f, 0.f};
         }
@@ -509,19 +543,16 @@ struct Pol32S : Pol32 {
     static __device__ __forceinline__ void network(const Consts &k, Tables &T, bool mine)
     {
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (!mine) {
-            uint32_t *row = reinterpret_cast<uint32_t *>(T.xrow[warp] + lane * 16);
-#pragma unroll
-            for (int j = 0; j < 8; j++) row[j] = 0u;
-        }
-        warp_mlp(k.mlp, T.xrow[warp], T.yrow[warp]);
+        if (!mine) *reinterpret_cast<uint4 *>(T.rows[warp] + lane * 16) = make_uint4(0u, 0u, 0u, 0u);
+        warp_mlp(k.mlp, T.rows[warp]);
     }
     static __device__ __forceinline__ Tau<float> finish(const icy_SimParams &P, const Consts &k, const Tables &T,
                                                         St &s, float &p_tr, float &q_tr, unsigned &accepted,
                                                         unsigned &exact)
     {
         const SurrogateOut o =
-            surrogate_finish(P, k, T.yrow[threadIdx.x >> 5] + (threadIdx.x & 31) * 4, s.H, s.Jp, s.d);
+            surrogate_finish(P, k, reinterpret_cast<const float *>(T.rows[threadIdx.x >> 5] + (threadIdx.x & 31) * 16),
+                             s.H, s.Jp);
         s.H = o.H;
         s.Jp = o.Jp;
         p_tr = o.p_tr;
@@ -876,13 +907,6 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                     __syncwarp();
                 }
         };
-        struct Deferred {
-            int p;
-            typename Pol::St s;
-            real v0, v1, B[4];
-            decltype(Pol::St::Jp) jp_old;
-            uint32_t meta_old;
-        } dfr;
         bool deferred = false;
         if (r < cnt) {
             const int p = s_wgbase[warp][k] + 32 * r + lane;
@@ -962,10 +986,13 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                 real p_tr, q_tr;
                 int redo;
                 tau = Pol::advance(P, K, s_tab, s, v0, v1, B, p_tr, q_tr, redo);
-                if (Pol::kSurrogate && redo == 2) {
-                    deferred = true;
-                    dfr = {p, s, v0, v1, {B[0], B[1], B[2], B[3]}, jp_old, meta_old};
-                } else {
+                if constexpr (Pol::kSurrogate) {
+                    if (redo == 2) {
+                        deferred = true;
+                        Pol::defer_save(s_tab, p, s, v0, v1, B, jp_old, meta_old);
+                    }
+                }
+                if (!deferred) {
                     redo_count += redo;
                     Pol::store(A, p, s, jp_old, meta_old);
                     if (R.record_pq) A.pq[p] = {p_tr, q_tr};
@@ -990,16 +1017,21 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                 }
                 Pol::network(K, s_tab, deferred);
                 if (deferred) {
+                    int dp;
+                    typename Pol::St ds;
+                    real dv0, dv1, dB[4], djp;
+                    uint32_t dmeta;
+                    Pol::defer_load(s_tab, A, dp, ds, dv0, dv1, dB, djp, dmeta);
                     real p_tr, q_tr;
-                    const Tau<real> t2 = Pol::finish(P, K, s_tab, dfr.s, p_tr, q_tr, mlp_ok, mlp_fb);
+                    const Tau<real> t2 = Pol::finish(P, K, s_tab, ds, p_tr, q_tr, mlp_ok, mlp_fb);
                     redo_count += 1;
-                    Pol::store(A, dfr.p, dfr.s, dfr.jp_old, dfr.meta_old);
-                    if (R.record_pq) A.pq[dfr.p] = {p_tr, q_tr};
+                    Pol::store(A, dp, ds, djp, dmeta);
+                    if (R.record_pq) A.pq[dp] = {p_tr, q_tr};
                     if (MODE == kModeFinal) {
-                        A.vel[dfr.p] = {dfr.v0, dfr.v1};
-                        A.Bp[dfr.p] = {dfr.B[0], dfr.B[1], dfr.B[2], dfr.B[3]};
+                        A.vel[dp] = {dv0, dv1};
+                        A.Bp[dp] = {dB[0], dB[1], dB[2], dB[3]};
                     }
-                    if (MODE != kModeFinal) p2g(dfr.s, dfr.v0, dfr.v1, dfr.B, t2);
+                    if (MODE != kModeFinal) p2g(ds, dv0, dv1, dB, t2);
                 }
             }
         }
@@ -1048,7 +1080,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
 // earlier launches, heaviest first, which the hardware dispatches first --
 // instead of letting late heavy tiles form the tail of the launch.
 template <class Pol, int TX, int TY, int MODE>
-__global__ void __launch_bounds__(256) k_tile_substep(const __grid_constant__ icy_SimParams P,
+__global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep(const __grid_constant__ icy_SimParams P,
                                                       const __grid_constant__ typename Pol::Consts K,
                                                       const typename Pol::Parts A, const __grid_constant__ TileRun R)
 {

@@ -356,20 +356,20 @@ __global__ void k_mlp_adam(float *net, float *m, float *v, const float *grad, in
 // the warp form over a batch (tests and measurements of the in-kernel form)
 __global__ void __launch_bounds__(128) k_mlp_warp_infer(const MlpWarpNet *N, const float *X, int n, float *Yout)
 {
-    __shared__ __align__(16) __nv_bfloat16 xrow[4][32 * 16];
-    __shared__ float yrow[4][32 * 4];
+    __shared__ __align__(16) unsigned char rows[4][32 * 16];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r = (blockIdx.x * 4 + warp) * 32 + lane;
+    __nv_bfloat16 *xrow = reinterpret_cast<__nv_bfloat16 *>(rows[warp]);
 #pragma unroll
-    for (int k = 0; k < 16; k++) {
+    for (int k = 0; k < 8; k++) {
         float v = 0.f;
         if (k < kMlpIn && r < n) v = (X[(size_t)r * kMlpIn + k] - N->x_mu[k]) * N->x_isd[k];
-        xrow[warp][lane * 16 + k] = __float2bfloat16(v);
+        xrow[lane * 8 + k] = __float2bfloat16(v);
     }
-    warp_mlp(N, xrow[warp], yrow[warp]);
+    warp_mlp(N, rows[warp]);
+    const float *yrow = reinterpret_cast<const float *>(rows[warp]);
     if (r < n)
-        for (int o = 0; o < kMlpOut; o++)
-            Yout[(size_t)r * kMlpOut + o] = yrow[warp][lane * 4 + o] * N->y_sd[o] + N->y_mu[o];
+        for (int o = 0; o < kMlpOut; o++) Yout[(size_t)r * kMlpOut + o] = yrow[lane * 4 + o] * N->y_sd[o] + N->y_mu[o];
 }
 
 // harvested trial states (H00, H01, H10, H11, Jp_inv, meta word) ->

@@ -86,6 +86,16 @@ __device__ __forceinline__ uint32_t ldg_u32(const __nv_bfloat16 *p)
     return __ldg(reinterpret_cast<const unsigned int *>(p));
 }
 
+// GELU of the warp form, on the hardware tanh approximation (tanh.approx.f32,
+// relative error about 2^-11, below the BF16 rounding the activation gets)
+__device__ __forceinline__ float gelu_fast(float z)
+{
+    const float c = 0.7978845608028654f, a = 0.044715f;
+    float th, u = c * (z + a * z * z * z);
+    asm("tanh.approx.f32 %0, %1;" : "=f"(th) : "f"(u));
+    return 0.5f * z * (1.0f + th);
+}
+
 // D += A B for one m16n8k16 tile (BF16 in, FP32 accumulate)
 __device__ __forceinline__ void mma_bf16_16816(float d[4], const uint32_t a[4], uint32_t b0, uint32_t b1)
 {
@@ -95,25 +105,27 @@ __device__ __forceinline__ void mma_bf16_16816(float d[4], const uint32_t a[4], 
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// One warp evaluates the network on 32 rows: xrow[lane] holds 16 BF16
-// normalised inputs of the lane's row (zeros past the sixth), and the 3
-// normalised outputs of row r come back in yrow[r][0..2]. Warp-collective:
-// every lane of the warp calls it. A layer's accumulator tiles (two
-// adjacent 8-column tiles) are the next layer's input fragment, so the
-// activations stay in registers; weights are read through L1 from N.
-static __device__ __noinline__ void warp_mlp(const MlpWarpNet *__restrict__ N, const __nv_bfloat16 *xrow,
-                                             float *yrow)
+// One warp evaluates the network on 32 rows. row points at 32 rows of 16
+// bytes: on entry row r holds the 8 BF16 normalised inputs of row r (the 6
+// features, then zeros; inputs 8-15 of the K = 16 fragment are zero and not
+// stored), on return its first 3 floats are the normalised outputs.
+// Warp-collective: every lane of the warp calls it. A layer's accumulator
+// tiles (two adjacent 8-column tiles) are the next layer's input fragment,
+// so the activations stay in registers; weights are read through L1 from N.
+static __device__ __noinline__ void warp_mlp(const MlpWarpNet *__restrict__ N, unsigned char *row)
 {
+    const __nv_bfloat16 *xrow = reinterpret_cast<const __nv_bfloat16 *>(row);
+    float *yrow = reinterpret_cast<float *>(row);
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     __syncwarp();
 #pragma unroll 1
     for (int mt = 0; mt < 2; mt++) {
         const int r0 = mt * 16 + g, r1 = r0 + 8;
         uint32_t a1[4];
-        a1[0] = *reinterpret_cast<const uint32_t *>(xrow + r0 * 16 + 2 * t);
-        a1[1] = *reinterpret_cast<const uint32_t *>(xrow + r1 * 16 + 2 * t);
-        a1[2] = *reinterpret_cast<const uint32_t *>(xrow + r0 * 16 + 2 * t + 8);
-        a1[3] = *reinterpret_cast<const uint32_t *>(xrow + r1 * 16 + 2 * t + 8);
+        a1[0] = *reinterpret_cast<const uint32_t *>(xrow + r0 * 8 + 2 * t);
+        a1[1] = *reinterpret_cast<const uint32_t *>(xrow + r1 * 8 + 2 * t);
+        a1[2] = 0u;
+        a1[3] = 0u;
         // layer 1 -> layer-2 input fragments (4 K-tiles of 16 hidden units)
         uint32_t a2[4][4];
 #pragma unroll
@@ -126,10 +138,10 @@ static __device__ __noinline__ void warp_mlp(const MlpWarpNet *__restrict__ N, c
                 c[h][0] = bb0; c[h][1] = bb1; c[h][2] = bb0; c[h][3] = bb1;
                 mma_bf16_16816(c[h], a1, ldg_u32(N->W1 + n * 16 + 2 * t), ldg_u32(N->W1 + n * 16 + 2 * t + 8));
             }
-            a2[kt][0] = pack_bf16(gelu(c[0][0]), gelu(c[0][1]));
-            a2[kt][1] = pack_bf16(gelu(c[0][2]), gelu(c[0][3]));
-            a2[kt][2] = pack_bf16(gelu(c[1][0]), gelu(c[1][1]));
-            a2[kt][3] = pack_bf16(gelu(c[1][2]), gelu(c[1][3]));
+            a2[kt][0] = pack_bf16(gelu_fast(c[0][0]), gelu_fast(c[0][1]));
+            a2[kt][1] = pack_bf16(gelu_fast(c[0][2]), gelu_fast(c[0][3]));
+            a2[kt][2] = pack_bf16(gelu_fast(c[1][0]), gelu_fast(c[1][1]));
+            a2[kt][3] = pack_bf16(gelu_fast(c[1][2]), gelu_fast(c[1][3]));
         }
         // layer 2, 16 hidden units at a time, streamed into layer 3
         float c3[4];
@@ -151,14 +163,15 @@ static __device__ __noinline__ void warp_mlp(const MlpWarpNet *__restrict__ N, c
                                    ldg_u32(N->W2 + n * 64 + 16 * kt + 2 * t + 8));
             }
             uint32_t a3[4];
-            a3[0] = pack_bf16(gelu(c[0][0]), gelu(c[0][1]));
-            a3[1] = pack_bf16(gelu(c[0][2]), gelu(c[0][3]));
-            a3[2] = pack_bf16(gelu(c[1][0]), gelu(c[1][1]));
-            a3[3] = pack_bf16(gelu(c[1][2]), gelu(c[1][3]));
+            a3[0] = pack_bf16(gelu_fast(c[0][0]), gelu_fast(c[0][1]));
+            a3[1] = pack_bf16(gelu_fast(c[0][2]), gelu_fast(c[0][3]));
+            a3[2] = pack_bf16(gelu_fast(c[1][0]), gelu_fast(c[1][1]));
+            a3[3] = pack_bf16(gelu_fast(c[1][2]), gelu_fast(c[1][3]));
             mma_bf16_16816(c3, a3, ldg_u32(N->W3 + g * 64 + 16 * k3 + 2 * t),
                            ldg_u32(N->W3 + g * 64 + 16 * k3 + 2 * t + 8));
         }
-        if (t < 2) {  // outputs 2t, 2t+1 (only 0..2 are real)
+        __syncwarp();  // every lane has read its inputs of this tile
+        if (t < 2) {  // outputs 2t, 2t+1 (only 0..2 are real), over the inputs
             yrow[r0 * 4 + 2 * t] = c3[0];
             yrow[r0 * 4 + 2 * t + 1] = c3[1];
             yrow[r1 * 4 + 2 * t] = c3[2];

@@ -18,7 +18,8 @@ def _crushing_case():
 
 
 def _run(p, soa, form, n, net=None, tol=0.02, harvest=0):
-    m = gpu_model(p, soa, form)
+    # the surrogate form runs 128-thread blocks (its per-warp scratch)
+    m = gpu_model(p, soa, form, threads=128)
     if net is not None:
         sg.set_surrogate(m.gpu, net, tol)
     if harvest:
@@ -103,7 +104,11 @@ def test_trained_surrogate_in_the_substep():
 @pytest.mark.gpu
 def test_surrogate_form_needs_a_network():
     p, soa = _crushing_case()
-    m = gpu_model(p, soa, im.FORM_FP32_SURROGATE)
+    m = gpu_model(p, soa, im.FORM_FP32_SURROGATE, threads=128)
     with pytest.raises(RuntimeError, match="without a network"):
+        m.gpu.run_substeps(m.prms, 2)
+    sg.set_surrogate(m.gpu, sg.init_net(0))
+    m.gpu.set_tile(1, 256)
+    with pytest.raises(RuntimeError, match="at most 128 threads"):
         m.gpu.run_substeps(m.prms, 2)
     m.gpu.close()
