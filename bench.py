@@ -55,6 +55,8 @@ def parse():
     a.add_argument("--no-cpu", action="store_true")
     a.add_argument("--no-fp64", action="store_true")
     a.add_argument("--no-surrogate", action="store_true")
+    a.add_argument("--no-ensemble", action="store_true")
+    a.add_argument("--ensemble-substeps", type=int, default=1000)
     a.add_argument("--form", choices=["fp32", "fp64"], default="fp32",
                    help="fused form of the headline (fp64: for profiling the FP64 fused kernel)")
     return a.parse_args()
@@ -519,6 +521,12 @@ def main():
                 },
             }
 
+    # --- the 64-case ensemble: every case as its own run_substeps (one after
+    # another, and all at once on their own streams) against one ensemble
+    # launch per substep over all cases' active tiles
+    if not args.no_ensemble and rank == 0 and world == 1:
+        extra["ensemble"] = ensemble_section(args, local, flush)
+
     # --- end to end: one frame through the public API with host buffers
     e2e = None
     if not args.no_e2e:
@@ -585,6 +593,104 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def ensemble_section(args, device, flush):
+    import torch
+
+    import icempm_b200 as im
+    from icempm_b200 import autotune, configs
+    from icempm_b200.ensemble import Ensemble
+
+    S = args.ensemble_substeps
+    cases = configs.c4_cases()
+    t0 = time.perf_counter()
+    models = [configs.c4_model(c, device) for c in cases]
+    npts = int(sum(m.prms.nPts for m in models))
+    t_setup = time.perf_counter() - t0
+    form = im.FORM_FP32
+    tile, threads, note = autotune.choose_ensemble(models, form, "c4_64", substeps=10)
+    for m in models:
+        m.gpu.set_form(form)
+        m.gpu.set_tile(tile, threads)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    # every case alone, one after another (each timed on its own stream)
+    for m in models:
+        m.gpu.run_substeps(m.prms, 4)
+    for m in models:
+        m.gpu.synchronize()
+    torch.cuda.synchronize()
+    seq_ms = 0.0
+    for m in models:
+        st = torch.cuda.ExternalStream(m.gpu.stream_handle())
+        with torch.cuda.stream(st):
+            flush.zero_()
+        a, b = ev(), ev()
+        a.record(st)
+        m.gpu.run_substeps(m.prms, S)
+        b.record(st)
+        b.synchronize()
+        seq_ms += a.elapsed_time(b)
+    # every case on its own stream, all enqueued before any finishes
+    torch.cuda.synchronize()
+    a, b = ev(), ev()
+    a.record()
+    for m in models:
+        st = torch.cuda.ExternalStream(m.gpu.stream_handle())
+        st.wait_event(a)
+        m.gpu.run_substeps(m.prms, S)
+    for m in models:
+        e = ev()
+        e.record(torch.cuda.ExternalStream(m.gpu.stream_handle()))
+        torch.cuda.current_stream().wait_event(e)
+    b.record()
+    b.synchronize()
+    conc_ms = a.elapsed_time(b)
+
+    ens = Ensemble(form, tile, threads, device=device)
+    for m in models:
+        ens.add(m)
+    ens.run(S)  # warm-up: descriptors, active tiles, the captured segments
+    ens.synchronize()
+    st = torch.cuda.ExternalStream(ens.stream_handle())
+    steps = 2
+    evs = [(ev(), ev()) for _ in range(steps)]
+    for k in range(steps):
+        with torch.cuda.stream(st):
+            flush.zero_()
+        evs[k][0].record(st)
+        ens.run(S)
+        evs[k][1].record(st)
+    ens.synchronize()
+    ens_ms = sum(x.elapsed_time(y) for x, y in evs) / steps
+    for m in models:
+        m.gpu.cuda_transfer_from_device()
+    for m in models:
+        m.gpu.synchronize()
+    errs = [int(m.gpu.error_code) for m in models]
+    ens.close()
+    for m in models:
+        m.gpu.close()
+    rate = npts * S / (ens_ms / 1e3)
+    return {
+        "workload": f"{len(cases)} indentation cases (seeded blocks of {min(m_.prms.nPts for m_ in models)}-"
+                    f"{max(m_.prms.nPts for m_ in models)} particles, {npts} in all; grid "
+                    f"{configs.C4['grid'][0]}x{configs.C4['grid'][1]} each; materials and indenters vary), FP32 form",
+        "value": rate, "unit": UNIT, "substeps": S,
+        "ms_per_substep": ens_ms / S,
+        "sequential_ms_per_substep": seq_ms / S,
+        "concurrent_streams_ms_per_substep": conc_ms / S,
+        "speedup_vs_sequential": seq_ms / ens_ms,
+        "speedup_vs_concurrent_streams": conc_ms / ens_ms,
+        "tile": im.TILE_VARIANTS[tile], "threads": threads, "tile_choice": note,
+        "timing": f"{steps} ensemble runs of {S} substeps (re-binned every 200, segments replayed from CUDA "
+                  "graphs), L2 flushed before each; the per-case arms run the same substeps through run_substeps",
+        "gpu_launches_per_substep": 1,
+        "setup_s": t_setup, "error_words": sorted(set(errs)),
+    }
 
 
 class _Null:

@@ -73,3 +73,53 @@ def active_nodes(p: SimParams, soa: np.ndarray) -> int:
         for j in range(3):
             mark[np.clip(by + j, 0, p.GridY + 2), np.clip(bx + i, 0, p.GridX + 2)] = True
     return int(mark[: p.GridY, : p.GridX].sum())
+
+
+# Ensemble of indentation cases: 64 cases on a 4 m x 1 m domain at
+# h = 1/256 (1024 x 256 grid), dt 1e-6, 5,000 substeps. Per case: particle
+# count log-uniform in [20k, 500k] (4 per cell), block aspect from a width
+# U[0.5, 2.0] m and height U[0.2, 0.6] m (the block is then sized to the
+# count), indenter speed U[0.05, 1.0] m/s, radius U[0.05, 0.2] m, friction
+# angle U[45, 70] deg, Young's modulus U[5e8, 3e9] Pa.
+C4 = dict(cases=64, grid=(1024, 256), dim=4.0, dt=1e-6, substeps=5000)
+
+
+def c4_cases(cases: int = 64, seed: int = 12345, n_min: int = 20_000, n_max: int = 500_000):
+    """Seeded case descriptions: (parameter overrides, cells_x, cells_y,
+    indenter height above the block bottom)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    gx, gy = C4["grid"]
+    out = []
+    for _ in range(cases):
+        n = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+        w, hgt = rng.uniform(0.5, 2.0), rng.uniform(0.2, 0.6)
+        cells = n / 4.0
+        cy = max(8, int(round(np.sqrt(cells * hgt / w))))
+        cx = int(round(cells / cy))
+        # keep the block inside the domain with room for the indenter
+        cx = min(cx, gx - 120)
+        cy = min(cy, gy - 40)
+        r = rng.uniform(0.05, 0.2)
+        over = dict(IndVelocity=float(rng.uniform(0.05, 1.0)), IndDiameter=float(2 * r),
+                    DP_phi=float(rng.uniform(45, 70)), YoungsModulus=float(rng.uniform(5e8, 3e9)))
+        h = C4["dim"] / gx
+        ind_y = min(0.5 * cy * h, r + 0.05)
+        out.append((over, cx, cy, ind_y))
+    return out
+
+
+def c4_model(case, device: int = 0, seed: int = 12345) -> Model:
+    """A Model holding one ensemble case (block loaded, constants set)."""
+    over, cx, cy, ind_y = case
+    gx, gy = C4["grid"]
+    m = Model(device)
+    p = SimParams()
+    p.Reset()
+    p.ParseString(json.dumps(dict(MATERIAL, GridX=gx, GridY=gy, GridXDimension=C4["dim"],
+                                  InitialTimeStep=C4["dt"], **over)))
+    m.prms = p
+    m.gpu.model = m
+    m.load_block(cx, cy, ind_y_above_floor=ind_y, grain_size=0.05, seed=seed)
+    return m

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <string>
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/icempm.h"
@@ -128,6 +129,7 @@ struct icm_ctx {
     bool ref_valid = true, internal_valid = false, internal_pq = false;
     int internal_variant = -1;
     int nslots = 0;
+    int *h_ns = nullptr;  // pinned: the slot count a re-binning reads back
     Binning bin;
     Fused fz;
 };
@@ -465,6 +467,10 @@ static int ensure_spare(icm_ctx *c, size_t nslots)
 {
     if (c->fz.spare_cap >= nslots) return ICM_OK;
     free_spare(c);
+    // headroom: the slot count changes a little at every re-binning, and a
+    // reallocation (cudaFree synchronises the device) costs far more than
+    // the memory
+    nslots += nslots / 4 + 4096;
     int rc;
     if ((rc = dalloc(&c->fz.spare_pid, nslots)) || (rc = dalloc(&c->fz.slot_key, nslots))) return rc;
     if (c->fz.form == ICM_FORM_FP64) {
@@ -485,15 +491,17 @@ static int ensure_spare(icm_ctx *c, size_t nslots)
 }
 
 // Re-bins the internal (slot-ordered) particle arrays by their current base
-// nodes. Only valid between steady-state launches of a run.
-static int rebin_internal(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
+// nodes. Only valid between steady-state launches of a run. Two halves: the
+// first ends with the new slot count on its way to c->h_ns, the second
+// (after the caller synchronised c->stream) gathers into the new layout.
+static int rebin_begin(icm_ctx *c, const icy_SimParams &P)
 {
     TileGeom g;
     int ntiles;
     geometry(P, c->internal_variant, g, ntiles);
     const size_t ncells = (size_t)ntiles * g.TX * g.TY;
     const int ngroups = (int)(ncells / 32);
-    const int ns_old = c->nslots, n = P.nPts;
+    const int ns_old = c->nslots;
     cudaStream_t s = c->stream;
     int rc = ensure_spare(c, (size_t)std::max(ns_old, 1));
     if (rc) return rc;
@@ -523,9 +531,26 @@ static int rebin_internal(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
     k_group_slots<<<(ngroups + 255) / 256, 256, 0, s>>>(ngroups, c->bin.cell_start, c->bin.group_slots);
     ICM_LAUNCHED("k_group_slots");
     if ((rc = scan_ints(c, c->bin.group_slots, ngroups, c->bin.gchunk, c->bin.group_base))) return rc;
-    int ns_new = 0;
-    ICM_CUDA(cudaMemcpyAsync(&ns_new, c->bin.group_base + ngroups, sizeof(int), cudaMemcpyDeviceToHost, s));
-    ICM_CUDA(cudaStreamSynchronize(s));
+    if (!c->h_ns && cudaMallocHost((void **)&c->h_ns, sizeof(int)) != cudaSuccess) {
+        c->h_ns = nullptr;
+        return icm::fail(ICM_ERR_NOMEM, "re-binning: pinned slot count");
+    }
+    ICM_CUDA(cudaMemcpyAsync(c->h_ns, c->bin.group_base + ngroups, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return ICM_OK;
+}
+
+static int rebin_finish(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
+{
+    TileGeom g;
+    int ntiles;
+    geometry(P, c->internal_variant, g, ntiles);
+    const size_t ncells = (size_t)ntiles * g.TX * g.TY;
+    const int ns_old = c->nslots, n = P.nPts;
+    cudaStream_t s = c->stream;
+    const Consts32 K32 = make_consts32(P);
+    const Pol64::Consts K64{0};
+    int rc;
+    const int ns_new = *c->h_ns;
     if ((size_t)ns_new > c->fz.spare_cap) {
         // the spare set must hold the new layout; grow it (contents of the
         // current set are untouched)
@@ -560,6 +585,14 @@ static int rebin_internal(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
     c->bin.cap_slots = c->fz.cap_pts;
     c->nslots = ns_new;
     return ICM_OK;
+}
+
+static int rebin_internal(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
+{
+    int rc = rebin_begin(c, P);
+    if (rc) return rc;
+    ICM_CUDA(cudaStreamSynchronize(c->stream));
+    return rebin_finish(c, P, keep_pq);
 }
 
 // Tile order for the next launches: by the costs measured on this tile
@@ -775,6 +808,7 @@ extern "C" int icm_destroy(icm_ctx *c)
     free_binning(c);
     dfree(c->d_pts); dfree(c->d_grid); dfree(c->d_bins); dfree(c->d_err); dfree(c->d_hist); dfree(c->d_redo); dfree(c->d_strays);
     dfree(c->d_mlp); dfree(c->d_mlp_counts); dfree(c->d_harvest); dfree(c->d_harvest_n);
+    if (c->h_ns) cudaFreeHost(c->h_ns);
     for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
     if (c->ev_start) cudaEventDestroy(c->ev_start);
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
@@ -1094,6 +1128,511 @@ extern "C" int icm_kernel_time(icm_ctx *c, double *total_ms, long long *launches
 }
 
 extern "C" void *icm_stream(icm_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+// ------------------------------------------------------------ ensembles
+
+struct icm_ensemble {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int form = ICM_FORM_FP32, variant = 1, threads = 128, rebin_interval = 200;
+    bool graphs = true;
+    std::vector<icm_ctx *> cases;
+    void *d_cases = nullptr;
+    size_t cases_bytes = 0;
+    int *d_tile_case = nullptr, *d_tile_local = nullptr, *d_nactive = nullptr, *d_seg_base = nullptr;
+    size_t tiles_cap = 0;
+    int nactive = 0;
+    double *d_ind_x = nullptr;
+    size_t ind_x_cap = 0;
+    uint8_t *d_active = nullptr;  // every case's tile mask, concatenated
+    size_t active_cap = 0;
+    std::vector<size_t> active_off;
+    struct Seg {
+        cudaGraphExec_t exec;
+        int len, grid;
+    };
+    std::vector<Seg> graphs_by_len;  // captured segments (at most kEnsGraphs lengths)
+    std::vector<cudaEvent_t> events;  // one per case, plus one for the ensemble stream
+    unsigned char *h_stage = nullptr;  // pinned: every case's tile starts, costs and dirty flags
+    size_t stage_cap = 0;
+};
+
+namespace {
+
+// a captured graph holds the descriptor and active-tile pointers: drop it
+// when they are reallocated (after cudaFree's implicit synchronisation)
+void ens_drop_graph(icm_ensemble *e)
+{
+    for (auto &g : e->graphs_by_len) cudaGraphExecDestroy(g.exec);
+    e->graphs_by_len.clear();
+}
+
+constexpr int kEnsGraphs = 4;
+
+template <class Pol, int TX, int TY, int MODE>
+int ens_launch_one(icm_ensemble *e, int grid, const void *d_cases, const EnsLaunch &L)
+{
+    constexpr int RN = (TX + 4) * (TY + 4);
+    const int nwarps = e->threads / 32;
+    const size_t dyn = tile_dyn_bytes<Pol, MODE>(RN, nwarps);
+    static size_t opted = 0;
+    if (dyn > opted) {
+        ICM_CUDA(cudaFuncSetAttribute(k_tile_substep_ens<Pol, TX, TY, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)dyn));
+        opted = dyn;
+    }
+    if (grid < 1) return ICM_OK;
+    k_tile_substep_ens<Pol, TX, TY, MODE><<<grid, e->threads, dyn, e->stream>>>(
+        static_cast<const EnsCase<Pol> *>(d_cases), L);
+    ICM_LAUNCHED("k_tile_substep_ens");
+    return ICM_OK;
+}
+
+template <class Pol, int TX, int TY>
+int ens_launch_tile(icm_ensemble *e, int mode, int grid, const void *d_cases, const EnsLaunch &L)
+{
+    switch (mode) {
+    case kModeP2GOnly: return ens_launch_one<Pol, TX, TY, kModeP2GOnly>(e, grid, d_cases, L);
+    case kModeFull: return ens_launch_one<Pol, TX, TY, kModeFull>(e, grid, d_cases, L);
+    default: return ens_launch_one<Pol, TX, TY, kModeFinal>(e, grid, d_cases, L);
+    }
+}
+
+template <class Pol>
+int ens_launch_variant(icm_ensemble *e, int mode, int grid, const void *d_cases, const EnsLaunch &L)
+{
+    switch (e->variant) {
+    case 0: return ens_launch_tile<Pol, 16, 8>(e, mode, grid, d_cases, L);
+    case 1: return ens_launch_tile<Pol, 16, 16>(e, mode, grid, d_cases, L);
+    case 2: return ens_launch_tile<Pol, 32, 8>(e, mode, grid, d_cases, L);
+    default: return ens_launch_tile<Pol, 32, 16>(e, mode, grid, d_cases, L);
+    }
+}
+
+int ens_launch(icm_ensemble *e, int mode, int grid, int j)
+{
+    EnsLaunch L{e->d_seg_base, j, e->d_tile_case, e->d_tile_local, e->d_nactive};
+    return e->form == ICM_FORM_FP64 ? ens_launch_variant<Pol64>(e, mode, grid, e->d_cases, L)
+                                    : ens_launch_variant<Pol32>(e, mode, grid, e->d_cases, L);
+}
+
+// e->stream waits for the cases' streams (to = true) or they for it
+int ens_join(icm_ensemble *e, bool to_ensemble)
+{
+    const size_t nc = e->cases.size();
+    if (to_ensemble) {
+        for (size_t i = 0; i < nc; i++) {
+            ICM_CUDA(cudaEventRecord(e->events[i], e->cases[i]->stream));
+            ICM_CUDA(cudaStreamWaitEvent(e->stream, e->events[i], 0));
+        }
+    } else {
+        ICM_CUDA(cudaEventRecord(e->events[nc], e->stream));
+        for (size_t i = 0; i < nc; i++) ICM_CUDA(cudaStreamWaitEvent(e->cases[i]->stream, e->events[nc], 0));
+    }
+    return ICM_OK;
+}
+
+template <class Pol>
+int ens_upload_cases(icm_ensemble *e, const std::vector<icy_SimParams> &P, icy_SimParams *const *p, int n)
+{
+    const size_t nc = e->cases.size();
+    std::vector<EnsCase<Pol>> hc(nc);
+    for (size_t i = 0; i < nc; i++) {
+        icm_ctx *c = e->cases[i];
+        EnsCase<Pol> &d = hc[i];
+        std::memset(&d, 0, sizeof(d));
+        d.P = P[i];
+        if constexpr (std::is_same<Pol, Pol64>::value) {
+            d.K = Pol64::Consts{0};
+            d.A = c->fz.p64;
+        } else {
+            d.K = make_consts32(P[i]);
+            d.A = c->fz.p32;
+        }
+        TileGeom g;
+        int ntiles;
+        geometry(P[i], e->variant, g, ntiles);
+        d.R.ntx = g.ntx;
+        d.R.nty = g.nty;
+        d.R.tile_start = c->bin.tile_start;
+        for (int b = 0; b < 3; b++) {
+            d.R.dirty[b] = c->fz.dirty + (size_t)b * ntiles;
+            d.R.grid[b] = c->fz.grid[b];
+        }
+        d.R.bins = c->d_bins;
+        d.R.err = c->d_err;
+        d.R.fp64_redo = c->d_redo;
+        d.R.cell_start = c->bin.cell_start;
+        d.R.group_base = c->bin.group_base;
+        d.R.strays = c->d_strays;
+        d.R.ind_y = p[i]->indenter_y;
+        d.R.cost = c->fz.cost;
+        d.hist = c->d_hist;
+        d.ind_x = e->d_ind_x + (size_t)i * n;
+        d.active = e->d_active + e->active_off[i];
+        d.step0 = p[i]->SimulationStep;
+        d.every = p[i]->UpdateEveryNthStep;
+        d.ntiles = ntiles;
+    }
+    const size_t bytes = sizeof(EnsCase<Pol>) * nc;
+    if (bytes > e->cases_bytes) {
+        if (e->d_cases) cudaFree(e->d_cases);
+        ens_drop_graph(e);
+        e->d_cases = nullptr;
+        if (cudaMalloc(&e->d_cases, bytes) != cudaSuccess) return icm::fail(ICM_ERR_NOMEM, "ensemble: descriptors");
+        e->cases_bytes = bytes;
+    }
+    ICM_CUDA(cudaMemcpyAsync(e->d_cases, hc.data(), bytes, cudaMemcpyHostToDevice, e->stream));
+    return ICM_OK;
+}
+
+// Active tiles: those holding particles, their eight neighbours (the nodes
+// their particles scatter to until the next re-binning) and any tile with a
+// dirty flag (its nodes still need zeroing or an update). The launch list
+// puts the tiles of all cases in descending order of the cost their last
+// full launch measured, so the heaviest (contact, crushed zones) start
+// first.
+int ens_active_tiles(icm_ensemble *e, const std::vector<icy_SimParams> &P)
+{
+    struct Item {
+        unsigned cost;
+        int c, t;
+    };
+    const size_t nc = e->cases.size();
+    // stage every case's tile starts (ntiles + 1 ints), costs (ntiles) and
+    // dirty flags (3 ntiles bytes, padded to 4) with one synchronisation
+    std::vector<size_t> off(nc + 1, 0);
+    std::vector<int> nt(nc);
+    std::vector<TileGeom> geo(nc);
+    for (size_t i = 0; i < nc; i++) {
+        geometry(P[i], e->variant, geo[i], nt[i]);
+        off[i + 1] = off[i] + 4 * ((size_t)nt[i] + 1) + 4 * (size_t)nt[i] + ((3 * (size_t)nt[i] + 3) & ~(size_t)3);
+    }
+    if (off[nc] > e->stage_cap) {
+        if (e->h_stage) cudaFreeHost(e->h_stage);
+        e->h_stage = nullptr;
+        e->stage_cap = 0;
+        if (cudaMallocHost((void **)&e->h_stage, off[nc]) != cudaSuccess) {
+            e->h_stage = nullptr;
+            return icm::fail(ICM_ERR_NOMEM, "ensemble: pinned staging");
+        }
+        e->stage_cap = off[nc];
+    }
+    for (size_t i = 0; i < nc; i++) {
+        icm_ctx *c = e->cases[i];
+        unsigned char *b = e->h_stage + off[i];
+        const size_t n = (size_t)nt[i];
+        ICM_CUDA(cudaMemcpyAsync(b, c->bin.tile_start, 4 * (n + 1), cudaMemcpyDeviceToHost, e->stream));
+        ICM_CUDA(cudaMemcpyAsync(b + 4 * (n + 1), c->fz.cost, 4 * n, cudaMemcpyDeviceToHost, e->stream));
+        ICM_CUDA(cudaMemcpyAsync(b + 8 * n + 4, c->fz.dirty, 3 * n, cudaMemcpyDeviceToHost, e->stream));
+    }
+    ICM_CUDA(cudaStreamSynchronize(e->stream));
+    std::vector<Item> items;
+    std::vector<uint8_t> mask;
+    e->active_off.assign(nc, 0);
+    for (size_t i = 0; i < nc; i++) {
+        const int ntiles = nt[i];
+        const TileGeom &g = geo[i];
+        const unsigned char *b = e->h_stage + off[i];
+        const int *ts = reinterpret_cast<const int *>(b);
+        const unsigned *cost = reinterpret_cast<const unsigned *>(b + 4 * ((size_t)ntiles + 1));
+        const uint8_t *dirty = b + 8 * (size_t)ntiles + 4;
+        e->active_off[i] = mask.size();
+        mask.resize(mask.size() + (size_t)ntiles, 0);
+        uint8_t *busy = mask.data() + e->active_off[i];
+        for (int t = 0; t < ntiles; t++) {
+            if (dirty[t] | dirty[(size_t)ntiles + t] | dirty[2 * (size_t)ntiles + t]) busy[t] = 1;
+            if (ts[t + 1] == ts[t]) continue;
+            const int tx = t % g.ntx, ty = t / g.ntx;
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int x = tx + dx, y = ty + dy;
+                    if (x >= 0 && y >= 0 && x < g.ntx && y < g.nty) busy[(size_t)y * g.ntx + x] = 1;
+                }
+        }
+        for (int t = 0; t < ntiles; t++)
+            if (busy[t]) items.push_back({cost[t], (int)i, t});
+    }
+    std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) { return a.cost > b.cost; });
+    std::vector<int> tc(items.size()), tl(items.size());
+    for (size_t k = 0; k < items.size(); k++) {
+        tc[k] = items[k].c;
+        tl[k] = items[k].t;
+    }
+    const size_t m = items.size();
+    int rc;
+    if (m > e->tiles_cap) {
+        dfree(e->d_tile_case);
+        dfree(e->d_tile_local);
+        ens_drop_graph(e);
+        if ((rc = dalloc(&e->d_tile_case, m)) || (rc = dalloc(&e->d_tile_local, m))) return rc;
+        e->tiles_cap = m;
+    }
+    if (mask.size() > e->active_cap) {
+        dfree(e->d_active);
+        if ((rc = dalloc(&e->d_active, mask.size()))) return rc;
+        e->active_cap = mask.size();
+    }
+    e->nactive = (int)m;
+    if (m) {
+        ICM_CUDA(cudaMemcpyAsync(e->d_tile_case, tc.data(), sizeof(int) * m, cudaMemcpyHostToDevice, e->stream));
+        ICM_CUDA(cudaMemcpyAsync(e->d_tile_local, tl.data(), sizeof(int) * m, cudaMemcpyHostToDevice, e->stream));
+    }
+    if (!mask.empty()) ICM_CUDA(cudaMemcpyAsync(e->d_active, mask.data(), mask.size(), cudaMemcpyHostToDevice, e->stream));
+    ICM_CUDA(cudaMemcpyAsync(e->d_nactive, &e->nactive, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    ICM_CUDA(cudaStreamSynchronize(e->stream));  // the host vectors go out of scope
+    return ICM_OK;
+}
+
+int ens_upload(icm_ensemble *e, const std::vector<icy_SimParams> &P, icy_SimParams *const *p, int n)
+{
+    const int rc = ens_active_tiles(e, P);
+    if (rc) return rc;
+    return e->form == ICM_FORM_FP64 ? ens_upload_cases<Pol64>(e, P, p, n) : ens_upload_cases<Pol32>(e, P, p, n);
+}
+
+int ens_check(icm_ensemble *e)
+{
+    const int nc = (int)e->cases.size();
+    if (e->form == ICM_FORM_FP64)
+        k_ens_check<Pol64><<<nc, 128, 0, e->stream>>>(static_cast<const EnsCase<Pol64> *>(e->d_cases));
+    else
+        k_ens_check<Pol32><<<nc, 128, 0, e->stream>>>(static_cast<const EnsCase<Pol32> *>(e->d_cases));
+    ICM_LAUNCHED("k_ens_check");
+    return ICM_OK;
+}
+
+// A replayable segment: len full-substep launches reading their substep
+// index from d_seg_base, over the current launch list (CTAs past *nactive
+// return, so a graph captured for a longer list stays valid).
+int ens_segment_graph(icm_ensemble *e, int len, cudaGraphExec_t &out)
+{
+    for (auto &g : e->graphs_by_len)
+        if (g.len == len && g.grid >= e->nactive) {
+            out = g.exec;
+            return ICM_OK;
+        }
+    for (size_t i = 0; i < e->graphs_by_len.size(); i++)
+        if (e->graphs_by_len[i].len == len || (int)e->graphs_by_len.size() >= kEnsGraphs) {
+            cudaGraphExecDestroy(e->graphs_by_len[i].exec);
+            e->graphs_by_len.erase(e->graphs_by_len.begin() + i);
+            break;
+        }
+    // set the kernel's shared-memory attribute outside the capture (grid 0 launches nothing)
+    int rc0 = ens_launch(e, kModeFull, 0, 0);
+    if (rc0) return rc0;
+    cudaGraph_t g = nullptr;
+    ICM_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = ICM_OK;
+    for (int j = 0; j < len && !rc; j++) rc = ens_launch(e, kModeFull, e->nactive, j);
+    const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess) return icm::fail(ICM_ERR_CUDA, std::string("ensemble capture: ") + cudaGetErrorString(ce));
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return icm::fail(ICM_ERR_CUDA, std::string("ensemble graph: ") + cudaGetErrorString(ie));
+    e->graphs_by_len.push_back({ex, len, e->nactive});
+    out = ex;
+    return ICM_OK;
+}
+
+}  // namespace
+
+extern "C" int icm_ensemble_destroy(icm_ensemble *e);
+
+extern "C" int icm_ensemble_create(icm_ensemble **out, int device, int form, int tile_variant, int threads)
+{
+    if (!out) return icm::fail(ICM_ERR_ARG, "icm_ensemble_create: null out");
+    *out = nullptr;
+    if (form != ICM_FORM_FP32 && form != ICM_FORM_FP64)
+        return icm::fail(ICM_ERR_ARG, "icm_ensemble_create: the fused FP32 or FP64 form");
+    if (tile_variant < 0 || tile_variant > 3 || threads < 32 || threads > 256 || threads % 32)
+        return icm::fail(ICM_ERR_ARG, "icm_ensemble_create: tile variant 0..3, threads 32..256 in warps");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return icm::fail(ICM_ERR_NODEVICE, "No avaialble CUDA devices");
+    if (device < 0 || device >= count) return icm::fail(ICM_ERR_ARG, "icm_ensemble_create: device index out of range");
+    const TileVariant tv = kVariants[tile_variant];
+    if (tv.TX * tv.TY > 32 * kMaxGroupsPerWarp * (threads / 32))
+        return icm::fail(ICM_ERR_ARG, "tile too large for the block size (need threads >= TX*TY/4)");
+    ICM_CUDA(cudaSetDevice(device));
+    icm_ensemble *e = new icm_ensemble();
+    e->device = device;
+    e->form = form;
+    e->variant = tile_variant;
+    e->threads = threads;
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc((void **)&e->d_nactive, sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void **)&e->d_seg_base, sizeof(int)) != cudaSuccess) {
+        icm_ensemble_destroy(e);
+        return icm::fail(ICM_ERR_CUDA, "icm_ensemble_create: stream/allocation failed");
+    }
+    *out = e;
+    return ICM_OK;
+}
+
+extern "C" int icm_ensemble_destroy(icm_ensemble *e)
+{
+    if (!e) return ICM_OK;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    ens_drop_graph(e);
+    for (cudaEvent_t ev : e->events) cudaEventDestroy(ev);
+    if (e->d_cases) cudaFree(e->d_cases);
+    dfree(e->d_tile_case);
+    dfree(e->d_tile_local);
+    dfree(e->d_nactive);
+    dfree(e->d_seg_base);
+    dfree(e->d_ind_x);
+    dfree(e->d_active);
+    if (e->h_stage) cudaFreeHost(e->h_stage);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return ICM_OK;
+}
+
+extern "C" int icm_ensemble_add(icm_ensemble *e, icm_ctx *c)
+{
+    if (!e || !c) return icm::fail(ICM_ERR_ARG, "icm_ensemble_add: null argument");
+    if (c->device != e->device) return icm::fail(ICM_ERR_ARG, "icm_ensemble_add: the case is on another device");
+    if (!c->d_pts) return icm::fail(ICM_ERR_STATE, "icm_ensemble_add: the case has no arrays (icm_allocate_arrays)");
+    for (icm_ctx *x : e->cases)
+        if (x == c) return icm::fail(ICM_ERR_ARG, "icm_ensemble_add: case added twice");
+    int rc = icm_set_form(c, e->form);
+    if (rc) return rc;
+    if ((rc = icm_set_tile(c, e->variant, e->threads))) return rc;
+    cudaEvent_t ev;
+    ICM_CUDA(cudaSetDevice(e->device));
+    ICM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    if (e->events.empty()) {
+        cudaEvent_t ev2;
+        ICM_CUDA(cudaEventCreateWithFlags(&ev2, cudaEventDisableTiming));
+        e->events.push_back(ev2);  // the ensemble stream's, kept last
+    }
+    e->events.insert(e->events.end() - 1, ev);
+    e->cases.push_back(c);
+    return ICM_OK;
+}
+
+extern "C" int icm_ensemble_size(icm_ensemble *e) { return e ? (int)e->cases.size() : -1; }
+
+extern "C" int icm_ensemble_set(icm_ensemble *e, int rebin_interval, int use_graphs)
+{
+    if (!e || rebin_interval < 0) return icm::fail(ICM_ERR_ARG, "icm_ensemble_set: bad argument");
+    e->rebin_interval = rebin_interval;
+    e->graphs = use_graphs != 0;
+    return ICM_OK;
+}
+
+extern "C" void *icm_ensemble_stream(icm_ensemble *e) { return e ? (void *)e->stream : nullptr; }
+
+extern "C" int icm_ensemble_run(icm_ensemble *e, icy_SimParams *const *p, int n)
+{
+    if (!e || !p) return icm::fail(ICM_ERR_ARG, "icm_ensemble_run: null argument");
+    if (n < 1) return icm::fail(ICM_ERR_ARG, "icm_ensemble_run: n < 1");
+    const size_t nc = e->cases.size();
+    if (nc == 0) return icm::fail(ICM_ERR_STATE, "icm_ensemble_run: no cases");
+    ICM_CUDA(cudaSetDevice(e->device));
+    int rc;
+    std::vector<icy_SimParams> P(nc);
+    std::vector<double> ind_x(nc * (size_t)n);
+    std::vector<double> t_end(nc);
+    std::vector<char> any_pq(nc, 0);
+    for (size_t i = 0; i < nc; i++) {
+        icm_ctx *c = e->cases[i];
+        if (!p[i]) return icm::fail(ICM_ERR_ARG, "icm_ensemble_run: null SimParams");
+        if ((rc = check_params(c, p[i]))) return rc;
+        if (c->form != e->form || c->tile_variant != e->variant || c->threads != e->threads)
+            return icm::fail(ICM_ERR_STATE, "icm_ensemble_run: a case's form or tile was changed after icm_ensemble_add");
+        P[i] = kernel_params(c, p[i]);
+        if (!c->internal_valid || c->fz.form != storage_form(c->form) || c->internal_variant != c->tile_variant) {
+            if ((rc = ensure_ref(c)) || (rc = pack(c, P[i]))) return rc;
+        }
+        TileGeom g;
+        int ntiles;
+        geometry(P[i], e->variant, g, ntiles);
+        const size_t nnodes = (size_t)P[i].GridX * P[i].GridY;
+        const size_t node_bytes = (storage_form(c->form) == ICM_FORM_FP64) ? sizeof(Node64) : sizeof(float4);
+        for (int b = 0; b < 3; b++) ICM_CUDA(cudaMemsetAsync(c->fz.grid[b], 0, node_bytes * nnodes, c->stream));
+        ICM_CUDA(cudaMemsetAsync(c->fz.dirty, 0, 3 * (size_t)ntiles, c->stream));
+        if ((rc = ensure_hist(c, n))) return rc;
+        ICM_CUDA(cudaMemsetAsync(c->d_hist, 0, sizeof(double) * 2 * (size_t)n, c->stream));
+        c->hist_n = n;
+        if (c->fz.cost_variant != c->tile_variant || c->fz.cost_ntiles != ntiles) {
+            ICM_CUDA(cudaMemsetAsync(c->fz.cost, 0, sizeof(unsigned) * (size_t)ntiles, c->stream));
+            c->fz.cost_variant = c->tile_variant;
+            c->fz.cost_ntiles = ntiles;
+        }
+        // the indenter path of Model::Step (model.cpp:20-25) for every substep
+        double t = p[i]->SimulationTime;
+        for (int k = 1; k <= n; k++) {
+            t += p[i]->InitialTimeStep;
+            ind_x[i * (size_t)n + k - 1] = p[i]->indenter_x_initial + t * p[i]->IndVelocity;
+            if ((p[i]->SimulationStep + k) % p[i]->UpdateEveryNthStep == 0) any_pq[i] = 1;
+        }
+        t_end[i] = t;
+    }
+    if ((rc = ens_join(e, true))) return rc;
+    if (ind_x.size() > e->ind_x_cap) {
+        dfree(e->d_ind_x);
+        if ((rc = dalloc(&e->d_ind_x, ind_x.size()))) return rc;
+        e->ind_x_cap = ind_x.size();
+    }
+    ICM_CUDA(cudaMemcpyAsync(e->d_ind_x, ind_x.data(), sizeof(double) * ind_x.size(), cudaMemcpyHostToDevice, e->stream));
+    if ((rc = ens_upload(e, P, p, n))) return rc;  // synchronises the ensemble stream
+
+    // prologue, full substeps in segments between re-binnings, final substep
+    if ((rc = ens_launch(e, kModeP2GOnly, e->nactive, 0))) return rc;
+    const int I = e->rebin_interval;
+    int k = 1;
+    while (k < n) {
+        int end = n - 1;  // last full substep of this segment
+        if (I > 0) end = std::min(end, ((k - 1) / I + 1) * I);
+        const int len = end - k + 1;
+        k_set_int<<<1, 1, 0, e->stream>>>(e->d_seg_base, k - 1);
+        ICM_LAUNCHED("k_set_int");
+        if (e->graphs && len > 1) {
+            cudaGraphExec_t ex = nullptr;
+            if ((rc = ens_segment_graph(e, len, ex))) return rc;
+            ICM_CUDA(cudaGraphLaunch(ex, e->stream));
+        } else {
+            for (int j = 0; j < len; j++)
+                if ((rc = ens_launch(e, kModeFull, e->nactive, j))) return rc;
+        }
+        k = end + 1;
+        if (I > 0 && end % I == 0 && end < n) {
+            // re-bin every case on its own stream, then refresh descriptors
+            if ((rc = ens_check(e)) || (rc = ens_join(e, false))) return rc;
+            for (size_t i = 0; i < nc; i++)
+                if ((rc = rebin_begin(e->cases[i], P[i]))) return rc;
+            for (size_t i = 0; i < nc; i++) ICM_CUDA(cudaStreamSynchronize(e->cases[i]->stream));
+            for (size_t i = 0; i < nc; i++) {
+                icm_ctx *c = e->cases[i];
+                if ((rc = rebin_finish(c, P[i], c->internal_pq || any_pq[i]))) return rc;
+            }
+            if ((rc = ens_join(e, true))) return rc;
+            if ((rc = ens_upload(e, P, p, n))) return rc;
+        }
+    }
+    k_set_int<<<1, 1, 0, e->stream>>>(e->d_seg_base, n - 1);
+    ICM_LAUNCHED("k_set_int");
+    if ((rc = ens_launch(e, kModeFinal, e->nactive, 0))) return rc;
+    if ((rc = ens_check(e)) || (rc = ens_join(e, false))) return rc;
+    for (size_t i = 0; i < nc; i++) {
+        icm_ctx *c = e->cases[i];
+        p[i]->SimulationStep += n;
+        p[i]->SimulationTime = t_end[i];
+        p[i]->indenter_x = ind_x[i * (size_t)n + n - 1];
+        c->internal_valid = true;
+        c->ref_valid = false;
+        c->internal_pq = c->internal_pq || any_pq[i];
+    }
+    return ICM_OK;
+}
 
 // ------------------------------------------------ learned projection
 

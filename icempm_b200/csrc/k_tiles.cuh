@@ -1097,6 +1097,90 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep(const __g
     }
 }
 
+// ---------------------------------------------------------- ensembles
+// Many cases (separate blocks, materials and indenters, each with its own
+// grid and particle arrays) advance together: one launch per substep covers
+// the active tiles of every case. A case's parameter block, constants,
+// particle arrays and the fixed part of its TileRun are read by each of its
+// CTAs into shared memory; everything that changes from substep to substep
+// is derived on the device from the substep index sidx = *seg_base + j, so
+// that one captured sequence of launches can be replayed for any segment.
+template <class Pol> struct EnsCase {
+    icy_SimParams P;
+    typename Pol::Consts K;
+    typename Pol::Parts A;
+    TileRun R;
+    double *hist;          // 2 doubles per substep of the run
+    const double *ind_x;   // indenter x after each substep of the run
+    const uint8_t *active; // 1 for each tile this case's launches cover
+    int step0, every;      // SimulationStep when the run started, UpdateEveryNthStep
+    int ntiles, pad;
+};
+
+struct EnsLaunch {
+    const int *seg_base;   // substep index of the first launch of the segment
+    int j;                 // this launch's place in the segment
+    const int *tile_case;  // active tiles: case and tile within the case
+    const int *tile_local;
+    const int *nactive;    // number of active tiles (CTAs past it return)
+};
+
+template <class Pol, int TX, int TY, int MODE>
+__global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const EnsCase<Pol> *__restrict__ cases,
+                                                                           const __grid_constant__ EnsLaunch L)
+{
+    __shared__ __align__(16) EnsCase<Pol> sc;
+    __shared__ long long s_clock;
+    if ((int)blockIdx.x >= *L.nactive) return;
+    const int c = L.tile_case[blockIdx.x], t = L.tile_local[blockIdx.x];
+    {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(cases + c);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(&sc);
+        for (int i = threadIdx.x; i < (int)(sizeof(EnsCase<Pol>) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (MODE == kModeP2GOnly) {
+            sc.R.bufA = sc.R.bufB = sc.R.bufC = 0;
+            sc.R.force_slot = nullptr;
+            sc.R.record_pq = 0;
+            sc.R.ind_x = sc.P.indenter_x;
+        } else {
+            const int sidx = *L.seg_base + L.j;
+            sc.R.bufA = sidx % 3;
+            sc.R.bufB = (sidx + 1) % 3;
+            sc.R.bufC = (sidx + 2) % 3;
+            sc.R.ind_x = sc.ind_x[sidx];
+            sc.R.force_slot = sc.hist + 2 * (size_t)sidx;
+            sc.R.record_pq = (sc.step0 + sidx + 1) % sc.every == 0 ? 1 : 0;
+            s_clock = clock64();
+        }
+    }
+    __syncthreads();
+    tile_body<Pol, TX, TY, MODE>(sc.P, sc.K, sc.A, sc.R, t);
+    if (MODE == kModeFull && sc.R.cost) {
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const long long dc = clock64() - s_clock;
+            sc.R.cost[t] = (unsigned)(dc < 0 ? 0 : (dc > 0xffffffffll ? 0xffffffffll : dc));
+        }
+    }
+}
+
+__global__ void k_set_int(int *dst, int value) { *dst = value; }
+
+// After a segment: a tile outside a case's active set whose dirty flag is
+// set received mass that no launch consumed (a particle drifted further
+// than a tile between re-binnings). Sets bit 2 of the case's error word.
+template <class Pol> __global__ void k_ens_check(const EnsCase<Pol> *__restrict__ cases)
+{
+    const EnsCase<Pol> &c = cases[blockIdx.x];
+    bool lost = false;
+    for (int t = threadIdx.x; t < c.ntiles; t += blockDim.x)
+        if (!c.active[t] && (c.R.dirty[0][t] | c.R.dirty[1][t] | c.R.dirty[2][t])) lost = true;
+    if (__syncthreads_or(lost) && threadIdx.x == 0) atomicOr(c.R.err, 2);
+}
+
 // Tile order by descending cost (ties by tile index): a bitonic sort of
 // (cost << 32 | ~tile) keys in shared memory, one CTA, n <= kMaxOrderTiles.
 constexpr int kMaxOrderTiles = 8192;

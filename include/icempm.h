@@ -248,6 +248,37 @@ int icm_set_harvest(icm_ctx *ctx, int capacity, int every);
  * record. */
 int icm_harvest_pairs(icm_ctx *ctx, const icy_SimParams *p, float *x, float *y, int cap, int *n_out);
 
+/* ------------------------------------------------------------ ensembles
+ * No counterpart in the reference. Many indentation cases -- each an
+ * icm_ctx with its own block, material, indenter, grid and particle
+ * arrays, set up as for icm_run_substeps -- advance together: every
+ * substep is one launch over the active tiles of all cases (tiles holding
+ * particles and their neighbours), the launches between re-binnings
+ * replayed from a captured CUDA graph. Results per case are those of
+ * icm_run_substeps on that case alone (same form and tile), up to the
+ * order of float atomics: icm_force_history, icm_transfer_from_device etc.
+ * read them from the case's context. */
+typedef struct icm_ensemble icm_ensemble;
+/* form: ICM_FORM_FP32 or ICM_FORM_FP64; tile_variant and threads as in
+ * icm_set_tile. */
+int icm_ensemble_create(icm_ensemble **out, int device, int form, int tile_variant, int threads);
+int icm_ensemble_destroy(icm_ensemble *e);
+/* Adds a case (arrays allocated, points uploaded); sets its form and tile
+ * to the ensemble's. The context stays the caller's. */
+int icm_ensemble_add(icm_ensemble *e, icm_ctx *ctx);
+int icm_ensemble_size(icm_ensemble *e);
+/* Re-binning interval in substeps (default 200; 0: only when a run
+ * starts) and whether segments are replayed from a CUDA graph (default 1). */
+int icm_ensemble_set(icm_ensemble *e, int rebin_interval, int use_graphs);
+/* n substeps of every case; p[i] is case i's SimParams, advanced as by
+ * icm_run_substeps. Asynchronous: the cases' streams wait for it. A case
+ * whose particles scattered into a tile outside its active set between two
+ * re-binnings (mass that no launch consumed; a shorter re-binning interval
+ * avoids it) gets bit 2 set in its error word (icm_transfer_from_device). */
+int icm_ensemble_run(icm_ensemble *e, icy_SimParams *const *p, int n);
+/* The ensemble's CUDA stream (cudaStream_t). */
+void *icm_ensemble_stream(icm_ensemble *e);
+
 /* ------------------------------------------------------------ snapshots
  * SnapshotManager (simulation/snapshotmanager.cpp) on the library's own
  * HDF5 reader and writer (no libhdf5); host-side, no device calls. Files

@@ -1,0 +1,150 @@
+"""Ensembles (icm_ensemble_*): many cases advanced by one launch per
+substep over all their active tiles, segments replayed from a CUDA graph.
+Each case must end where the same case run alone ends."""
+import numpy as np
+import pytest
+
+import icempm_b200 as im
+from icempm_b200 import configs
+from icempm_b200.ensemble import Ensemble
+
+from mpm_cases import compare_states, gpu_model, gpu_state, params, scene
+
+CASES = [  # (cells, seed, overrides)
+    ((40, 10), 3, dict(YoungsModulus=8e8, IndVelocity=0.5)),
+    ((24, 14), 5, dict(YoungsModulus=2e9, IndVelocity=1.0, DP_phi=50)),
+    ((56, 6), 9, dict(IndVelocity=0.2)),
+]
+
+
+def _case(cells, seed, over):
+    p = params(**over)
+    soa = scene(p, cells=cells, seed=seed, ind_y=0.03, vel=0.05, perturb=5e-4)
+    return p, soa
+
+
+def _alone(p, soa, form, n, rebin):
+    m = gpu_model(p, soa, form, tile=1, threads=128)
+    m.gpu.set_rebin_interval(rebin)
+    m.gpu.run_substeps(m.prms, n)
+    hist = m.gpu.force_history(n)
+    state = gpu_state(m)
+    prms = m.prms.copy()
+    m.gpu.close()
+    return prms, state, hist
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", [im.FORM_FP64, im.FORM_FP32])
+@pytest.mark.parametrize("graphs", [True, False])
+def test_ensemble_matches_cases_run_alone(form, graphs):
+    n, rebin = 13, 4
+    cases = [_case(*c) for c in CASES]
+    ens = Ensemble(form, tile=1, threads=128)
+    ens.set(rebin_interval=rebin, graphs=graphs)
+    models = []
+    for p, soa in cases:
+        m = gpu_model(p, soa, form, tile=1, threads=128)
+        ens.add(m)
+        models.append(m)
+    ens.run(n)
+    tol_pos, tol = (1e-9, 1e-9) if form == im.FORM_FP64 else (1e-5, 1e-4)
+    for (p, soa), m in zip(cases, models):
+        got, hist = gpu_state(m), m.gpu.force_history(n)
+        q, ref, href = _alone(p, soa, form, n, rebin)
+        assert m.prms.SimulationStep == q.SimulationStep and m.prms.SimulationTime == q.SimulationTime
+        assert m.prms.indenter_x == q.indenter_x
+        err = compare_states(p, got, ref, soa)
+        assert err["disp_h"] <= tol_pos and err["strain"] <= tol and err["vel"] <= tol, err
+        assert err["crushed_mismatch"] == 0
+        scale = max(np.abs(href).max(), 1e-30)
+        assert np.abs(hist - href).max() <= 1e3 * tol * scale
+        assert m.gpu.error_code == 0
+    ens.close()
+    for m in models:
+        m.gpu.close()
+
+
+@pytest.mark.gpu
+def test_ensemble_runs_compose():
+    """Two ensemble runs continue each other (a second run re-packs nothing
+    and reuses its captured graph)."""
+    cases = [_case(*c) for c in CASES[:2]]
+    ens = Ensemble(im.FORM_FP32, tile=1, threads=128)
+    ens.set(rebin_interval=4)
+    models = [gpu_model(p, soa, im.FORM_FP32, tile=1, threads=128) for p, soa in cases]
+    for m in models:
+        ens.add(m)
+    ens.run(9)
+    ens.run(9)
+    for (p, soa), m in zip(cases, models):
+        _, ref, _ = _alone(p, soa, im.FORM_FP32, 18, 4)
+        err = compare_states(p, gpu_state(m), ref, soa)
+        assert err["disp_h"] <= 1e-5 and err["strain"] <= 1e-4, err
+        assert m.prms.SimulationStep == 18
+    ens.close()
+    for m in models:
+        m.gpu.close()
+
+
+def test_ensemble_argument_errors():
+    with pytest.raises(RuntimeError):
+        Ensemble(im.FORM_FP64_STEPWISE)
+    with pytest.raises(RuntimeError):
+        Ensemble(im.FORM_FP32, tile=3, threads=32)  # 32x16 tile needs 128 threads
+
+
+def test_c4_cases():
+    cs = configs.c4_cases()
+    n = np.array([4 * cx * cy for _, cx, cy, _ in cs])
+    assert len(cs) == 64 and n.min() >= 19_000 and n.max() <= 500_000
+    assert 7e6 < n.sum() < 1e7
+    gx, gy = configs.C4["grid"]
+    assert all(cx < gx - 100 and cy < gy - 30 for _, cx, cy, _ in cs)
+    phis = [o["DP_phi"] for o, *_ in cs]
+    assert 45 <= min(phis) and max(phis) <= 70
+    assert cs == configs.c4_cases()  # seeded
+
+
+def _drifting_block(speed=600.0):
+    """A block translating at `speed` m/s: in 120 substeps of 2 us it moves
+    0.144 m, 18 cells, further than a 16 x 16 tile."""
+    p = params(YoungsModulus=1e9)
+    soa = scene(p, cells=(24, 8), seed=11, ind_y=0.03)
+    S = im.SoA(soa, p.nPtsPitch, p.nPts)
+    room_right = p.GridXDimension - S.pos[0].max()
+    S.vel[0] = speed if room_right > 0.3 else -speed
+    S.vel[1] = 0.0
+    return p, soa
+
+
+@pytest.mark.gpu
+def test_ensemble_flags_mass_outside_active_tiles():
+    """Without re-binning the drifting block scatters into tiles its launches
+    do not cover: the case's error word gets bit 2. Re-binning every 5
+    substeps keeps it covered and the run matches the block run alone."""
+    n = 120
+    p, soa = _drifting_block()
+    ens = Ensemble(im.FORM_FP32, tile=1, threads=128)
+    ens.set(rebin_interval=0)
+    m = gpu_model(p, soa, im.FORM_FP32, tile=1, threads=128)
+    ens.add(m)
+    ens.run(n)
+    m.gpu.cuda_transfer_from_device()
+    m.gpu.synchronize()
+    assert m.gpu.error_code & 2
+    ens.close()
+    m.gpu.close()
+
+    ens = Ensemble(im.FORM_FP32, tile=1, threads=128)
+    ens.set(rebin_interval=5)
+    m = gpu_model(p, soa, im.FORM_FP32, tile=1, threads=128)
+    ens.add(m)
+    ens.run(n)
+    got = gpu_state(m)
+    assert m.gpu.error_code == 0
+    _, ref, _ = _alone(p, soa, im.FORM_FP32, n, 5)
+    err = compare_states(p, got, ref, soa)
+    assert err["disp_h"] <= 1e-5 and err["vel"] <= 1e-4, err
+    ens.close()
+    m.gpu.close()
