@@ -57,6 +57,7 @@ def parse():
     a.add_argument("--no-surrogate", action="store_true")
     a.add_argument("--no-ensemble", action="store_true")
     a.add_argument("--ensemble-substeps", type=int, default=1000)
+    a.add_argument("--ensemble-cases", type=int, default=64)
     a.add_argument("--form", choices=["fp32", "fp64"], default="fp32",
                    help="fused form of the headline (fp64: for profiling the FP64 fused kernel)")
     return a.parse_args()
@@ -603,13 +604,13 @@ def ensemble_section(args, device, flush):
     from icempm_b200.ensemble import Ensemble
 
     S = args.ensemble_substeps
-    cases = configs.c4_cases()
+    cases = configs.c4_cases()[: args.ensemble_cases]
     t0 = time.perf_counter()
     models = [configs.c4_model(c, device) for c in cases]
     npts = int(sum(m.prms.nPts for m in models))
     t_setup = time.perf_counter() - t0
     form = im.FORM_FP32
-    tile, threads, note = autotune.choose_ensemble(models, form, "c4_64", substeps=10)
+    tile, threads, note = autotune.choose_ensemble(models, form, f"c4_{len(cases)}", substeps=10)
     for m in models:
         m.gpu.set_form(form)
         m.gpu.set_tile(tile, threads)
