@@ -37,6 +37,9 @@ SENS_NOISE = 3e-8  # std of the initial Fe perturbation of the FP64 sensitivity 
 LATE_SUBSTEPS = 200  # launches timed after a full frame (crushed particles present)
 # learned projection: pairs harvested from the 250k-particle workload
 HARVEST_CONFIG, HARVEST_EVERY, HARVEST_CAP = "c2_250k", 5, 4_000_000
+# more pairs, from cases with other materials and indenters: the first 16
+# cases of the ensemble workload, 3,000 substeps
+HARVEST_ENS_CASES, HARVEST_ENS_SUBSTEPS, HARVEST_ENS_CAP = 16, 3000, 1_000_000
 SUR_STEPS, SUR_TILES, SUR_TOL = 3000, 64, 0.02
 
 
@@ -477,6 +480,21 @@ def main():
             mh.gpu.run_substeps(mh.prms, configs.CONFIGS[HARVEST_CONFIG][6])
             xh, yh = sg.harvest_pairs(mh.gpu, mh.prms, HARVEST_CAP)
             mh.gpu.close()
+            from icempm_b200.ensemble import Ensemble
+
+            he = Ensemble(im.FORM_FP32, 1, 128, device=local)
+            hms = [configs.c4_model(c, local) for c in configs.c4_cases()[:HARVEST_ENS_CASES]]
+            for hm in hms:
+                sg.set_harvest(hm.gpu, HARVEST_ENS_CAP, HARVEST_EVERY)
+                he.add(hm)
+            he.run(HARVEST_ENS_SUBSTEPS)
+            n_c2 = len(xh)
+            parts = [sg.harvest_pairs(hm.gpu, hm.prms, HARVEST_ENS_CAP) for hm in hms]
+            he.close()
+            for hm in hms:
+                hm.gpu.close()
+            xh = np.concatenate([xh] + [a for a, _ in parts])
+            yh = np.concatenate([yh] + [b for _, b in parts])
             t1 = time.perf_counter()
             net, loss = sg.fit(xh, yh, steps=SUR_STEPS, batch_tiles=SUR_TILES, lr=3e-3, seed=0, device=local)
             t2 = time.perf_counter()
@@ -507,7 +525,10 @@ def main():
                 "roofline": {"achieved": a3, "frac": a3 / hbm, "avg_launch_us": 1e3 * k3ms / max(k3n, 1)},
                 "late_frame_us_per_launch": late_s,
                 "training": {"pairs": int(len(xh)), "harvested_from": f"{HARVEST_CONFIG}, FP32 form, every "
-                                                                       f"{HARVEST_EVERY} substeps of a 10,000-substep frame",
+                                                                       f"{HARVEST_EVERY} substeps of a 10,000-substep frame "
+                                                                       f"({n_c2} pairs), and the first {HARVEST_ENS_CASES} "
+                                                                       f"ensemble cases over {HARVEST_ENS_SUBSTEPS} substeps "
+                                                                       f"({len(xh) - n_c2} pairs)",
                              "steps": SUR_STEPS, "batch": 128 * SUR_TILES, "first_loss": float(loss[:10].mean()),
                              "final_loss": float(loss[-100:].mean()), "harvest_s": t1 - t0, "train_s": t2 - t1},
                 "tolerance": SUR_TOL,
@@ -597,6 +618,11 @@ def main():
 
 
 def ensemble_section(args, device, flush):
+    """The 64-case workload three ways, each arm on a fresh set of the same
+    seeded cases (same initial states, same substeps): every case's own
+    run_substeps one after another; all cases on their own streams at once;
+    one ensemble. The ensemble then continues to the workload's full
+    horizon (5,000 substeps)."""
     import torch
 
     import icempm_b200 as im
@@ -604,26 +630,43 @@ def ensemble_section(args, device, flush):
     from icempm_b200.ensemble import Ensemble
 
     S = args.ensemble_substeps
+    horizon = max(S, configs.C4["substeps"]) if args.ensemble_cases == configs.C4["cases"] else S
     cases = configs.c4_cases()[: args.ensemble_cases]
-    t0 = time.perf_counter()
-    models = [configs.c4_model(c, device) for c in cases]
-    npts = int(sum(m.prms.nPts for m in models))
-    t_setup = time.perf_counter() - t0
     form = im.FORM_FP32
-    tile, threads, note = autotune.choose_ensemble(models, form, f"c4_{len(cases)}", substeps=10)
-    for m in models:
-        m.gpu.set_form(form)
-        m.gpu.set_tile(tile, threads)
+    WARM = 3  # warm-up substeps of every arm (packing)
+
+    def fresh():
+        ms = [configs.c4_model(c, device) for c in cases]
+        for m in ms:
+            m.gpu.set_form(form)
+        return ms
+
+    def close(ms):
+        for m in ms:
+            m.gpu.close()
 
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
+    def warm(ms):
+        for m in ms:
+            m.gpu.set_tile(tile, threads)
+            m.gpu.run_substeps(m.prms, WARM)
+        for m in ms:
+            m.gpu.synchronize()
+        torch.cuda.synchronize()
+
+    t0 = time.perf_counter()
+    models = fresh()
+    npts = int(sum(m.prms.nPts for m in models))
+    sizes = (min(m.prms.nPts for m in models), max(m.prms.nPts for m in models))
+    t_setup = time.perf_counter() - t0
+    tile, threads, note = autotune.choose_ensemble(models, form, f"c4_{len(cases)}", substeps=10)
+    close(models)
+
     # every case alone, one after another (each timed on its own stream)
-    for m in models:
-        m.gpu.run_substeps(m.prms, 4)
-    for m in models:
-        m.gpu.synchronize()
-    torch.cuda.synchronize()
+    models = fresh()
+    warm(models)
     seq_ms = 0.0
     for m in models:
         st = torch.cuda.ExternalStream(m.gpu.stream_handle())
@@ -635,8 +678,12 @@ def ensemble_section(args, device, flush):
         b.record(st)
         b.synchronize()
         seq_ms += a.elapsed_time(b)
+    close(models)
+
     # every case on its own stream, all enqueued before any finishes
-    torch.cuda.synchronize()
+    models = fresh()
+    warm(models)
+    flush.zero_()
     a, b = ev(), ev()
     a.record()
     for m in models:
@@ -650,47 +697,53 @@ def ensemble_section(args, device, flush):
     b.record()
     b.synchronize()
     conc_ms = a.elapsed_time(b)
+    close(models)
 
+    # the ensemble: runs of S substeps up to the horizon; the first run
+    # covers the same substeps as the per-case arms
+    models = fresh()
     ens = Ensemble(form, tile, threads, device=device)
     for m in models:
         ens.add(m)
-    ens.run(S)  # warm-up: descriptors, active tiles, the captured segments
-    ens.synchronize()
     st = torch.cuda.ExternalStream(ens.stream_handle())
-    steps = 2
-    evs = [(ev(), ev()) for _ in range(steps)]
-    for k in range(steps):
+    ens.run(WARM)
+    ens.synchronize()
+    torch.cuda.synchronize()
+    runs = max(1, horizon // S)
+    evs = [(ev(), ev()) for _ in range(runs)]
+    for k in range(runs):
         with torch.cuda.stream(st):
             flush.zero_()
         evs[k][0].record(st)
         ens.run(S)
         evs[k][1].record(st)
     ens.synchronize()
-    ens_ms = sum(x.elapsed_time(y) for x, y in evs) / steps
+    run_ms = [x.elapsed_time(y) for x, y in evs]
+    ens_ms = run_ms[0]
     for m in models:
         m.gpu.cuda_transfer_from_device()
     for m in models:
         m.gpu.synchronize()
     errs = [int(m.gpu.error_code) for m in models]
     ens.close()
-    for m in models:
-        m.gpu.close()
-    rate = npts * S / (ens_ms / 1e3)
+    close(models)
     return {
-        "workload": f"{len(cases)} indentation cases (seeded blocks of {min(m_.prms.nPts for m_ in models)}-"
-                    f"{max(m_.prms.nPts for m_ in models)} particles, {npts} in all; grid "
-                    f"{configs.C4['grid'][0]}x{configs.C4['grid'][1]} each; materials and indenters vary), FP32 form",
-        "value": rate, "unit": UNIT, "substeps": S,
-        "ms_per_substep": ens_ms / S,
-        "sequential_ms_per_substep": seq_ms / S,
-        "concurrent_streams_ms_per_substep": conc_ms / S,
-        "speedup_vs_sequential": seq_ms / ens_ms,
-        "speedup_vs_concurrent_streams": conc_ms / ens_ms,
+        "workload": f"{len(cases)} indentation cases (seeded blocks of {sizes[0]}-{sizes[1]} particles, {npts} in "
+                    f"all; grid {configs.C4['grid'][0]}x{configs.C4['grid'][1]} each; materials and indenters "
+                    "vary), FP32 form",
+        "value": npts * runs * S / (sum(run_ms) / 1e3), "unit": UNIT, "substeps": runs * S,
+        "ms_per_substep": sum(run_ms) / (runs * S),
+        "ms_per_substep_by_run": [x / S for x in run_ms],
+        "first_run": {"substeps": S, "ensemble_ms_per_substep": ens_ms / S,
+                      "sequential_ms_per_substep": seq_ms / S, "concurrent_streams_ms_per_substep": conc_ms / S,
+                      "speedup_vs_sequential": seq_ms / ens_ms, "speedup_vs_concurrent_streams": conc_ms / ens_ms},
         "tile": im.TILE_VARIANTS[tile], "threads": threads, "tile_choice": note,
-        "timing": f"{steps} ensemble runs of {S} substeps (re-binned every 200, segments replayed from CUDA "
-                  "graphs), L2 flushed before each; the per-case arms run the same substeps through run_substeps",
+        "timing": f"every arm: fresh copies of the same cases, {WARM} warm-up substeps (packing), then timed runs "
+                  f"of {S} substeps (re-binned every 200), L2 flushed before each. Ensemble: {runs} runs, segments "
+                  "replayed from CUDA graphs (the first captures inside the first run); per-case arms: the first "
+                  "run, through run_substeps",
         "gpu_launches_per_substep": 1,
-        "setup_s": t_setup, "error_words": sorted(set(errs)),
+        "setup_s_per_copy": t_setup, "error_words": sorted(set(errs)),
     }
 
 

@@ -291,6 +291,9 @@ static int ensure_slots(icm_ctx *c, int form, size_t nslots)
     dfree(c->fz.p32.meta); dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
     dfree(c->bin.pid);
     free_spare(c);
+    // the same headroom as the spare set: re-binning swaps the two sets, and
+    // the slot count drifts a little with every re-binning
+    nslots += nslots / 4 + 4096;
     c->fz.form = form;
     c->fz.cap_pts = nslots;
     c->bin.cap_slots = nslots;
@@ -330,8 +333,11 @@ static int scan_ints(icm_ctx *c, const int *in, int n, int *chunk, int *out)
     return ICM_OK;
 }
 
+static int ensure_spare(icm_ctx *c, size_t nslots);
+
 // Bins the reference SoA by tile and base node and gathers it into the
-// internal arrays of form c->form.
+// internal arrays of form c->form (and makes sure the spare set that
+// re-binning gathers into exists, so that no run allocates).
 static int pack(icm_ctx *c, const icy_SimParams &P)
 {
     TileGeom g;
@@ -366,6 +372,7 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
     ICM_CUDA(cudaMemcpyAsync(&nslots, c->bin.group_base + ngroups, sizeof(int), cudaMemcpyDeviceToHost, s));
     ICM_CUDA(cudaStreamSynchronize(s));
     if ((rc = ensure_slots(c, storage_form(c->form), (size_t)std::max(nslots, 1)))) return rc;
+    if ((rc = ensure_spare(c, (size_t)std::max(nslots, 1)))) return rc;
     ICM_CUDA(cudaMemsetAsync(c->bin.pid, 0xff, sizeof(int) * (size_t)std::max(nslots, 1), s));
     if (n > 0) {
         if (storage_form(c->form) == ICM_FORM_FP64)
@@ -1248,6 +1255,12 @@ int ens_upload_cases(icm_ensemble *e, const std::vector<icy_SimParams> &P, icy_S
         } else {
             d.K = make_consts32(P[i]);
             d.A = c->fz.p32;
+            if (c->d_harvest && c->harvest_every > 0) {
+                d.K.harvest = c->d_harvest;
+                d.K.harvest_n = c->d_harvest_n;
+                d.K.harvest_cap = c->harvest_cap;
+                d.harvest_every = c->harvest_every;
+            }
         }
         TileGeom g;
         int ntiles;

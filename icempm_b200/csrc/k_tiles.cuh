@@ -108,6 +108,7 @@ template <class T> struct Tau { T t00, t01, t10, t11; };
 // the grain id (bits 0-15) and the crushed flag (bits 16-23).
 struct Pol64 {
     static constexpr bool kSurrogate = false;
+    static constexpr bool kHarvest = false;  // Consts has no harvest fields
     static constexpr int kMinBlocks = 0;
     // Bp from raw node velocities, operation order of the reference
     static constexpr bool kRelativeGradient = false;
@@ -216,6 +217,7 @@ struct Pol64 {
 // holds the grain's residues and the crushed flag (grain_meta32).
 struct Pol32 {
     static constexpr bool kSurrogate = false;
+    static constexpr bool kHarvest = true;
     static constexpr int kMinBlocks = 0;  // no residency hint: the compiler's own register choice
     // Bp = 4/h sum W (v_i - v_c) dpos^T with v_c the stencil's centre node:
     // equal to the reference's sum since sum W dpos = 0, but free of the
@@ -1114,8 +1116,17 @@ template <class Pol> struct EnsCase {
     const double *ind_x;   // indenter x after each substep of the run
     const uint8_t *active; // 1 for each tile this case's launches cover
     int step0, every;      // SimulationStep when the run started, UpdateEveryNthStep
-    int ntiles, pad;
+    int ntiles;
+    int harvest_every;     // FP32 form: substeps between harvests of crushed states (0: none)
 };
+
+// the harvest pointer of a launch that is not a harvest substep is cleared
+template <class Pol> __device__ __forceinline__ void ens_gate_harvest(EnsCase<Pol> &c, int sidx, bool on)
+{
+    if constexpr (Pol::kHarvest) {
+        if (!(on && c.harvest_every > 0 && (c.step0 + sidx + 1) % c.harvest_every == 0)) c.K.harvest = nullptr;
+    }
+}
 
 struct EnsLaunch {
     const int *seg_base;   // substep index of the first launch of the segment
@@ -1145,6 +1156,7 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const
             sc.R.force_slot = nullptr;
             sc.R.record_pq = 0;
             sc.R.ind_x = sc.P.indenter_x;
+            ens_gate_harvest(sc, 0, false);
         } else {
             const int sidx = *L.seg_base + L.j;
             sc.R.bufA = sidx % 3;
@@ -1153,6 +1165,7 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const
             sc.R.ind_x = sc.ind_x[sidx];
             sc.R.force_slot = sc.hist + 2 * (size_t)sidx;
             sc.R.record_pq = (sc.step0 + sidx + 1) % sc.every == 0 ? 1 : 0;
+            ens_gate_harvest(sc, sidx, true);
             s_clock = clock64();
         }
     }

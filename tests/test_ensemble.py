@@ -148,3 +148,41 @@ def test_ensemble_flags_mass_outside_active_tiles():
     assert err["disp_h"] <= 1e-5 and err["vel"] <= 1e-4, err
     ens.close()
     m.gpu.close()
+
+
+@pytest.mark.gpu
+def test_ensemble_harvest_matches_cases_run_alone():
+    """Crushed particles' trial states recorded every second substep inside
+    an ensemble are those each case records when run alone."""
+    from icempm_b200 import surrogate as sg
+
+    n, every, cap = 6, 2, 200000
+
+    def crushing(seed):
+        p = params()
+        return p, scene(p, seed=seed, perturb=2e-3, vel=0.05, crushed_frac=0.5, jp_spread=0.005)
+
+    cases = [crushing(3), crushing(8)]
+    ens = Ensemble(im.FORM_FP32, tile=1, threads=128)
+    models = []
+    for p, soa in cases:
+        m = gpu_model(p, soa, im.FORM_FP32, tile=1, threads=128)
+        sg.set_harvest(m.gpu, cap, every)
+        ens.add(m)
+        models.append(m)
+    ens.run(n)
+    for (p, soa), m in zip(cases, models):
+        x, y = sg.harvest_pairs(m.gpu, m.prms, cap)
+        a = gpu_model(p, soa, im.FORM_FP32, tile=1, threads=128)
+        sg.set_harvest(a.gpu, cap, every)
+        a.gpu.run_substeps(a.prms, n)
+        xa, ya = sg.harvest_pairs(a.gpu, a.prms, cap)
+        a.gpu.close()
+        assert len(xa) > 1000 and abs(len(x) - len(xa)) <= 0.005 * len(xa)
+        k = min(len(x), len(xa))
+        for col in range(3):
+            u, v = np.sort(x[:, col])[:k], np.sort(xa[:, col])[:k]
+            assert np.percentile(np.abs(u - v), 99) <= 1e-3
+    ens.close()
+    for m in models:
+        m.gpu.close()
