@@ -12,6 +12,7 @@
 // the internal arrays current; member-style kernels and transfers unpack
 // first. Nothing here falls back to the host: every failure is a status.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled (reached through the runtime, no libcuda link)
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -130,6 +131,13 @@ struct icm_ctx {
     int internal_variant = -1;
     int nslots = 0;
     int *h_ns = nullptr;  // pinned: the slot count a re-binning reads back
+    // TMA descriptors of the three grid buffers (device copy) and what they
+    // were encoded for
+    CUtensorMap *d_tmap = nullptr;
+    TmapSet h_tmap{};  // host copy: the kernel parameter of single runs
+    bool tmap_ok = false;
+    void *tmap_grid[3] = {nullptr, nullptr, nullptr};
+    int tmap_gx = -1, tmap_gy = -1, tmap_form = -1, tmap_variant = -1;
     Binning bin;
     Fused fz;
 };
@@ -439,7 +447,7 @@ static int launch_one(icm_ctx *c, int ntiles, const icy_SimParams &P, const type
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
         opted = dyn;
     }
-    k_tile_substep<Pol, TX, TY, MODE><<<ntiles, c->threads, dyn, c->stream>>>(P, K, A, R);
+    k_tile_substep<Pol, TX, TY, MODE><<<ntiles, c->threads, dyn, c->stream>>>(P, K, A, R, c->h_tmap);
     ICM_LAUNCHED("k_tile_substep");
     return ICM_OK;
 }
@@ -602,6 +610,68 @@ static int rebin_internal(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
     return rebin_finish(c, P, keep_pq);
 }
 
+// TMA descriptors of the grid buffers for the node-region copies of the
+// fused kernel: 2D maps of {4 GridX, GridY} floats (doubles in the FP64
+// form) with a box of {4 (TX+4), TY+4}. The runtime hands out the driver's
+// encoder; where it is missing or refuses, the kernel keeps its plain loads.
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+static int ensure_tmaps(icm_ctx *c, const icy_SimParams &P)
+{
+    const int form = storage_form(c->form);
+    if (c->tmap_form == form && c->tmap_variant == c->tile_variant && c->tmap_gx == P.GridX && c->tmap_gy == P.GridY &&
+        c->tmap_grid[0] == c->fz.grid[0] && c->tmap_grid[1] == c->fz.grid[1] && c->tmap_grid[2] == c->fz.grid[2])
+        return ICM_OK;
+    c->tmap_ok = false;
+    c->tmap_form = form;
+    c->tmap_variant = c->tile_variant;
+    c->tmap_gx = P.GridX;
+    c->tmap_gy = P.GridY;
+    for (int b = 0; b < 3; b++) c->tmap_grid[b] = c->fz.grid[b];
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+    if (!enc) return ICM_OK;
+    if (!c->d_tmap) {
+        if (cudaMalloc((void **)&c->d_tmap, 3 * sizeof(CUtensorMap)) != cudaSuccess) {
+            c->d_tmap = nullptr;
+            return icm::fail(ICM_ERR_NOMEM, "tensor maps");
+        }
+    }
+    const TileVariant tv = kVariants[c->tile_variant];
+    const size_t elem = (form == ICM_FORM_FP64) ? sizeof(double) : sizeof(float);
+    CUtensorMap h[3];
+    for (int b = 0; b < 3; b++) {
+        const cuuint64_t dims[2] = {4 * (cuuint64_t)P.GridX, (cuuint64_t)P.GridY};
+        const cuuint64_t strides[1] = {4 * elem * (cuuint64_t)P.GridX};
+        const cuuint32_t box[2] = {4 * (cuuint32_t)(tv.TX + 4), (cuuint32_t)(tv.TY + 4)};
+        const cuuint32_t es[2] = {1, 1};
+        const CUresult r = enc(&h[b], form == ICM_FORM_FP64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                               2, c->fz.grid[b], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return ICM_OK;
+    }
+    ICM_CUDA(cudaMemcpyAsync(c->d_tmap, h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    ICM_CUDA(cudaStreamSynchronize(c->stream));  // h goes out of scope
+    for (int b = 0; b < 3; b++) c->h_tmap.m[b] = h[b];
+    c->tmap_ok = true;
+    return ICM_OK;
+}
+
 // Tile order for the next launches: by the costs measured on this tile
 // geometry, or the identity (null) while there are none.
 static int tile_order(icm_ctx *c, int ntiles, const int *&order)
@@ -670,6 +740,8 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     R.ind_y = p->indenter_y;
     R.cost = c->fz.cost;
     if ((rc = tile_order(c, ntiles, R.order))) return rc;
+    if ((rc = ensure_tmaps(c, P))) return rc;
+    R.tmap = c->tmap_ok ? c->d_tmap : nullptr;
 
     Consts32 K32 = make_consts32(P);
     K32.mlp = c->d_mlp;
@@ -816,6 +888,7 @@ extern "C" int icm_destroy(icm_ctx *c)
     dfree(c->d_pts); dfree(c->d_grid); dfree(c->d_bins); dfree(c->d_err); dfree(c->d_hist); dfree(c->d_redo); dfree(c->d_strays);
     dfree(c->d_mlp); dfree(c->d_mlp_counts); dfree(c->d_harvest); dfree(c->d_harvest_n);
     if (c->h_ns) cudaFreeHost(c->h_ns);
+    if (c->d_tmap) cudaFree(c->d_tmap);
     for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
     if (c->ev_start) cudaEventDestroy(c->ev_start);
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
@@ -1280,6 +1353,7 @@ int ens_upload_cases(icm_ensemble *e, const std::vector<icy_SimParams> &P, icy_S
         d.R.strays = c->d_strays;
         d.R.ind_y = p[i]->indenter_y;
         d.R.cost = c->fz.cost;
+        d.R.tmap = c->tmap_ok ? c->d_tmap : nullptr;
         d.hist = c->d_hist;
         d.ind_x = e->d_ind_x + (size_t)i * n;
         d.active = e->d_active + e->active_off[i];
@@ -1580,6 +1654,7 @@ extern "C" int icm_ensemble_run(icm_ensemble *e, icy_SimParams *const *p, int n)
             c->fz.cost_variant = c->tile_variant;
             c->fz.cost_ntiles = ntiles;
         }
+        if ((rc = ensure_tmaps(c, P[i]))) return rc;
         // the indenter path of Model::Step (model.cpp:20-25) for every substep
         double t = p[i]->SimulationTime;
         for (int k = 1; k <= n; k++) {

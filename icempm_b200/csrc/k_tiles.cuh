@@ -44,9 +44,11 @@
 // c = m v - S_h (fx, fy)^T, which equals W_ij (m, m v + S dpos_ij).
 #pragma once
 #include <cstdint>
+#include <cuda.h>  // CUtensorMap (the type only)
 #include <cuda_pipeline.h>
 #include "mpm_math32.cuh"
 #include "mlp.cuh"
+#include "tc05.cuh"
 
 namespace icm {
 
@@ -90,7 +92,58 @@ struct TileRun {
     // substep launch writes tile t's clock cycles to cost[t]
     const int *order;
     unsigned *cost;
+    // TMA descriptors of the three grid buffers in global memory, or null
+    // (ensembles; a single run passes them as a kernel parameter)
+    const CUtensorMap *tmap;
 };
+
+// the TMA descriptors of the three grid buffers, as a kernel parameter
+struct TmapSet {
+    CUtensorMap m[3];
+};
+
+// error word bits: 1 a particle left the grid (the reference's flag),
+// 2 an ensemble case scattered outside its active tiles, 4 a tensor copy of
+// a node region did not complete in time
+constexpr int kErrTmaTimeout = 4;
+constexpr int kTmaPolls = 1 << 22;
+
+// Copies the (RX x RY)-node region at node (rx0, ry0) of one grid buffer
+// into shared memory with one 2D tensor copy; nodes outside the grid read as
+// zero. The x coordinate is 4 * rx0 elements of 4 (FP32) or 8 (FP64) bytes,
+// a multiple of 16 bytes for any rx0, negative ones included. Thread 0
+// issues the copy; every thread of the CTA must later call tma_region_wait
+// (the CTA may not exit with the copy in flight).
+__device__ __forceinline__ void tma_region_issue(const CUtensorMap *map, bool map_in_global, void *dst, int rx0,
+                                                 int ry0, uint32_t bytes, uint64_t *bar)
+{
+    if (threadIdx.x == 0) {
+        // a descriptor in global memory (written by a host copy) is fenced
+        // for the tensor-map proxy; one in kernel parameters needs nothing
+        if (map_in_global) asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+        tc05::mbar_init(bar, 1);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc05::smem_u32(bar)), "r"(bytes)
+                     : "memory");
+        asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                     "[%4];" ::"r"(tc05::smem_u32(dst)),
+                     "l"(map), "r"(4 * rx0), "r"(ry0), "r"(tc05::smem_u32(bar))
+                     : "memory");
+    }
+}
+
+// Waits for the copy; false (and kErrTmaTimeout raised) when it did not
+// complete within the poll limit.
+__device__ __forceinline__ bool tma_region_wait(uint64_t *bar, int *err)
+{
+    __syncthreads();  // the barrier was initialised before anyone polls it
+    bool ok = __syncthreads_and(tc05::mbar_wait(bar, 0, kTmaPolls));
+    if (!ok) {
+        // give the copy a second chance to land before the buffer is reused
+        __syncthreads_and(tc05::mbar_wait(bar, 0, kTmaPolls));
+        if (threadIdx.x == 0) atomicOr(err, kErrTmaTimeout);
+    }
+    return ok;
+}
 
 struct Parts64 { double2 *pos; double4 *F; double *Jp; uint32_t *meta; double2 *vel; double4 *Bp; double2 *pq; };
 struct Parts32 { uint32_t *cell; float2 *frac; float4 *H; float *Jp; uint32_t *meta; float2 *vel; float4 *Bp; float2 *pq; };
@@ -637,7 +690,8 @@ __host__ __device__ constexpr size_t tile_dyn_bytes(int RN, int nwarps)
 // uniform over the CTA.
 template <class Pol, int TX, int TY, int MODE>
 __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename Pol::Consts &K,
-                                          const typename Pol::Parts &A, const TileRun &R, const int t)
+                                          const typename Pol::Parts &A, const TileRun &R, const int t,
+                                          const CUtensorMap *tmaps, const bool tmaps_in_global)
 {
     using real = typename Pol::real;
     using V2 = typename Pol::V2;
@@ -646,8 +700,9 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     constexpr int RX = TX + 4, RY = TY + 4, RN = RX * RY;
     __shared__ V2 s_v[RN];
     // one private accumulation region per warp (dynamic shared memory)
-    extern __shared__ __align__(16) unsigned char s_dyn[];
+    extern __shared__ __align__(128) unsigned char s_dyn[];
     Acc *s_acc = reinterpret_cast<Acc *>(s_dyn);
+    __shared__ uint64_t s_tma_bar;
     __shared__ double s_bins[2 * kMaxBins];
     __shared__ double s_tot[2];
     __shared__ int s_contact, s_mark[9];
@@ -663,6 +718,17 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     const int tid = threadIdx.x, nthr = blockDim.x;
     Node *gA = (Node *)R.grid[R.bufA];
     Node *gB = (Node *)R.grid[R.bufB];
+    // a full substep of a tile with particles stages its node region with
+    // one tensor copy into the (not yet used) accumulation regions, issued
+    // here so that it lands while the tile zeroes and sets up
+    bool staging = false;
+    if constexpr (MODE == kModeFull) {
+        staging = p1 > p0 && tmaps && tile_region_bytes<Pol, MODE>(RN, nthr >> 5) >= RN * sizeof(Node) &&
+                  (tc05::smem_u32(s_dyn) & 127u) == 0;
+        if (staging)
+            tma_region_issue(tmaps + R.bufA, tmaps_in_global, s_dyn, rx0, ry0, (uint32_t)(RN * sizeof(Node)),
+                             &s_tma_bar);
+    }
 
     // 1. zero this tile in the buffer the next substep will scatter into;
     //    the flag is cleared only after every thread has read it
@@ -700,6 +766,8 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     // 2. grid update of the region (velocities into shared memory)
     if (MODE != kModeP2GOnly) {
         if (np > 0) {
+            const bool staged = staging && tma_region_wait(&s_tma_bar, R.err);
+            const Node *s_nodes = reinterpret_cast<const Node *>(s_dyn);
             // four nodes per thread per pass: their loads are issued together
             constexpr int NB = 4;
             for (int k0 = tid; k0 < RN; k0 += NB * nthr) {
@@ -708,7 +776,11 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                 for (int b = 0; b < NB; b++) {
                     const int k = k0 + b * nthr;
                     const int gx = rx0 + k % RX, gy = ry0 + k / RX;
-                    if (k < RN && gx >= 0 && gy >= 0 && gx < GX && gy < GY) nd[b] = gA[(size_t)gy * GX + gx];
+                    if (staged) {
+                        if (k < RN) nd[b] = s_nodes[k];
+                    } else if (k < RN && gx >= 0 && gy >= 0 && gx < GX && gy < GY) {
+                        nd[b] = gA[(size_t)gy * GX + gx];
+                    }
                 }
 #pragma unroll
                 for (int b = 0; b < NB; b++) {
@@ -755,6 +827,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         }
     }
     const int nwarps_blk = nthr >> 5;
+    if (MODE == kModeFull && tmaps) __syncthreads();  // the staged region is read before it is zeroed
     if (MODE != kModeFinal)
         for (int k = tid; k < RN * nwarps_blk; k += nthr) acc_zero(s_acc[k]);
     __syncthreads();
@@ -1084,12 +1157,13 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
 template <class Pol, int TX, int TY, int MODE>
 __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep(const __grid_constant__ icy_SimParams P,
                                                       const __grid_constant__ typename Pol::Consts K,
-                                                      const typename Pol::Parts A, const __grid_constant__ TileRun R)
+                                                      const typename Pol::Parts A, const __grid_constant__ TileRun R,
+                                                      const __grid_constant__ TmapSet T)
 {
     __shared__ long long s_clock;
     const int t = R.order ? R.order[blockIdx.x] : blockIdx.x;
     if (MODE == kModeFull && threadIdx.x == 0) s_clock = clock64();
-    tile_body<Pol, TX, TY, MODE>(P, K, A, R, t);
+    tile_body<Pol, TX, TY, MODE>(P, K, A, R, t, R.tmap ? T.m : nullptr, false);
     if (MODE == kModeFull && R.cost) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1170,7 +1244,7 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const
         }
     }
     __syncthreads();
-    tile_body<Pol, TX, TY, MODE>(sc.P, sc.K, sc.A, sc.R, t);
+    tile_body<Pol, TX, TY, MODE>(sc.P, sc.K, sc.A, sc.R, t, sc.R.tmap, true);
     if (MODE == kModeFull && sc.R.cost) {
         __syncthreads();
         if (threadIdx.x == 0) {
