@@ -447,7 +447,20 @@ static int launch_one(icm_ctx *c, int ntiles, const icy_SimParams &P, const type
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
         opted = dyn;
     }
-    k_tile_substep<Pol, TX, TY, MODE><<<ntiles, c->threads, dyn, c->stream>>>(P, K, A, R, c->h_tmap);
+    // programmatic dependent launch: the next substep's CTAs are launched
+    // while this one's last wave runs, and wait in the kernel (griddepcontrol)
+    // until it has completed
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ntiles);
+    cfg.blockDim = dim3(c->threads);
+    cfg.dynamicSmemBytes = dyn;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    ICM_CUDA(cudaLaunchKernelEx(&cfg, k_tile_substep<Pol, TX, TY, MODE>, P, K, A, R, c->h_tmap));
     ICM_LAUNCHED("k_tile_substep");
     return ICM_OK;
 }

@@ -1161,6 +1161,11 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep(const __g
                                                       const __grid_constant__ TmapSet T)
 {
     __shared__ long long s_clock;
+    // launched as a programmatic dependent: wait until the previous kernel
+    // of the stream has completed and its writes are visible, then let the
+    // next one launch (its CTAs take free slots and wait here in turn)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int t = R.order ? R.order[blockIdx.x] : blockIdx.x;
     if (MODE == kModeFull && threadIdx.x == 0) s_clock = clock64();
     tile_body<Pol, TX, TY, MODE>(P, K, A, R, t, R.tmap ? T.m : nullptr, false);
