@@ -1275,8 +1275,20 @@ int ens_launch_one(icm_ensemble *e, int grid, const void *d_cases, const EnsLaun
         opted = dyn;
     }
     if (grid < 1) return ICM_OK;
-    k_tile_substep_ens<Pol, TX, TY, MODE><<<grid, e->threads, dyn, e->stream>>>(
-        static_cast<const EnsCase<Pol> *>(d_cases), L);
+    // a programmatic dependent of the previous launch, as single runs are
+    // (inside a captured segment this becomes a programmatic graph edge)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(e->threads);
+    cfg.dynamicSmemBytes = dyn;
+    cfg.stream = e->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    ICM_CUDA(cudaLaunchKernelEx(&cfg, k_tile_substep_ens<Pol, TX, TY, MODE>, static_cast<const EnsCase<Pol> *>(d_cases),
+                                L));
     ICM_LAUNCHED("k_tile_substep_ens");
     return ICM_OK;
 }

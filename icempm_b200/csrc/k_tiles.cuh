@@ -1221,6 +1221,9 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const
 {
     __shared__ __align__(16) EnsCase<Pol> sc;
     __shared__ long long s_clock;
+    // programmatic dependent of the previous substep (see k_tile_substep)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if ((int)blockIdx.x >= *L.nactive) return;
     const int c = L.tile_case[blockIdx.x], t = L.tile_local[blockIdx.x];
     {
