@@ -416,6 +416,33 @@ def main():
             mm.gpu.kernel_timing(False)
             return 1e3 * kms2 / max(kn2, 1)
 
+        # the FP32 form's state against the FP64 fused form's after 1, 10 and
+        # 100 substeps from the same initial state
+        early = {}
+        pm = int(p0.nPtsPitch)
+        pair = [make(im.FORM_FP64, tile64, threads64), make(im.FORM_FP32, tile)]
+        done = 0
+        for target in (1, 10, 100):
+            bufs = []
+            for mm in pair:
+                mm.gpu.run_substeps(mm.prms, target - done)
+                mm.gpu.cuda_transfer_from_device()
+                mm.gpu.synchronize()
+                bufs.append(im.SoA(mm.gpu.tmp_transfer_buffer.copy(), pm, n))
+            done = target
+            a, b = bufs
+            dfe = np.abs(b.Fe - a.Fe).max(axis=0)
+            strain = np.abs(a.Fe - np.array([1.0, 0.0, 0.0, 1.0])[:, None]).max()
+            early[str(target)] = {
+                "x_max_err_h": float(np.abs(b.pos - a.pos).max() / p0.cellsize),
+                "v_rel_err": float(np.abs(b.vel - a.vel).max() / max(np.abs(a.vel).max(), 1e-30)),
+                "Fe_err_rel_to_max_strain": float(dfe.max() / max(strain, 1e-30)),
+                "Fe_err_p99_rel_to_max_strain": float(np.percentile(dfe, 99) / max(strain, 1e-30)),
+                "Jp_inv_max_abs_err": float(np.abs(b.Jp_inv - a.Jp_inv).max()),
+            }
+        for mm in pair:
+            mm.gpu.close()
+
         for form in (im.FORM_FP64, im.FORM_FP32, im.FORM_FP64_STEPWISE):
             mm = make(form, tile64 if form != im.FORM_FP32 else tile, threads64 if form != im.FORM_FP32 else None)
             mm.gpu.run_substeps(mm.prms, nsub)
@@ -456,6 +483,7 @@ def main():
         x32 = s32[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n]
         extra["accuracy"] = {
             "substeps": nsub, "against": "fp64 fused form on the GPU (parity-tested against the CPU FP64 oracle)",
+            "fp32_state_err_after_substeps": early,
             "peak_force_fp64_N": float(f64.max()), "peak_force_fp32_N": float(f32.max()),
             "peak_force_rel_err": float(abs(f32.max() - f64.max()) / max(f64.max(), 1e-30)),
             "force_history_rel_l2": float(np.linalg.norm(f32 - f64) / max(np.linalg.norm(f64), 1e-30)),
