@@ -181,6 +181,7 @@ def _lib():
                 "icm_fp64_redo_count": (i, [vp, C.POINTER(C.c_ulonglong)]),
                 "icm_stray_count": (i, [vp, C.POINTER(C.c_ulonglong)]),
                 "icm_set_rebin_interval": (i, [vp, i]),
+                "icm_set_tile_split": (i, [vp, i, d]),
                 "icm_record_start": (i, [vp]), "icm_record_stop": (i, [vp]),
                 "icm_elapsed_ms": (i, [vp, C.POINTER(C.c_float)]),
                 "icm_stream": (vp, [vp]),
@@ -385,6 +386,11 @@ class GPU_Implementation5:
     def set_rebin_interval(self, substeps: int) -> None:
         self.initialize()
         _check(_lib().icm_set_rebin_interval(self._ctx, substeps))
+
+    def set_tile_split(self, max_tiles: int = 128, ratio: float = 1.3) -> None:
+        """Heavy tiles run as two CTAs (icm_set_tile_split; max_tiles 0: off)."""
+        self.initialize()
+        _check(_lib().icm_set_tile_split(self._ctx, max_tiles, ratio))
 
     def stray_count(self) -> int:
         v = C.c_ulonglong(0)

@@ -99,6 +99,10 @@ struct icm_ctx {
     int form = ICM_FORM_FP64_STEPWISE;
     int tile_variant = 1, threads = 128;
     int rebin_interval = 200;
+    // heavy tiles run as two CTAs: at most split_max tiles whose measured
+    // cost exceeds split_ratio times the mean over tiles with particles
+    int split_max = 128;
+    double split_ratio = 1.3;
 
     icy_SimParams prms{};
     size_t cap_pts = 0, cap_nodes = 0, pts_pitch = 0, grid_pitch = 0;
@@ -261,8 +265,10 @@ static int ensure_grids(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t
                 c->fz.grid[b] = g;
             }
         }
-        if ((rc = dalloc(&c->fz.dirty, 3 * ntiles)) || (rc = dalloc(&c->fz.cost, ntiles)) ||
-            (rc = dalloc(&c->fz.order, ntiles)))
+        // cost: a tile's two halves; order: the tiles plus at most one
+        // extra CTA per tile (the second halves of split tiles)
+        if ((rc = dalloc(&c->fz.dirty, 3 * ntiles)) || (rc = dalloc(&c->fz.cost, 2 * ntiles)) ||
+            (rc = dalloc(&c->fz.order, 2 * ntiles)))
             return rc;
     }
     if (c->bin.cap_pts < npts || c->bin.cap_cells < ncells || c->bin.cap_tiles < ntiles) {
@@ -686,12 +692,14 @@ static int ensure_tmaps(icm_ctx *c, const icy_SimParams &P)
 }
 
 // Tile order for the next launches: by the costs measured on this tile
-// geometry, or the identity (null) while there are none.
-static int tile_order(icm_ctx *c, int ntiles, const int *&order)
+// geometry, the heaviest tiles split over two CTAs; or the identity (null)
+// while there are no costs. nlaunch: the grid of the fused launches.
+static int tile_order(icm_ctx *c, int ntiles, const int *&order, int &nlaunch)
 {
     order = nullptr;
+    nlaunch = ntiles;
     if (c->fz.cost_variant != c->tile_variant || c->fz.cost_ntiles != ntiles) {
-        ICM_CUDA(cudaMemsetAsync(c->fz.cost, 0, sizeof(unsigned) * (size_t)ntiles, c->stream));
+        ICM_CUDA(cudaMemsetAsync(c->fz.cost, 0, 2 * sizeof(unsigned) * (size_t)ntiles, c->stream));
         c->fz.cost_variant = c->tile_variant;
         c->fz.cost_ntiles = ntiles;
         return ICM_OK;
@@ -705,9 +713,12 @@ static int tile_order(icm_ctx *c, int ntiles, const int *&order)
                                       (int)(sizeof(unsigned long long) * kMaxOrderTiles)));
         opted = true;
     }
-    k_tile_order<<<1, kOrderThreads, sizeof(unsigned long long) * m, c->stream>>>(ntiles, c->fz.cost, c->fz.order);
+    const int max_split = std::min(std::max(c->split_max, 0), ntiles);
+    k_tile_order<<<1, kOrderThreads, sizeof(unsigned long long) * m, c->stream>>>(
+        ntiles, c->fz.cost, c->bin.tile_start, max_split, (float)c->split_ratio, c->fz.order);
     ICM_LAUNCHED("k_tile_order");
     order = c->fz.order;
+    nlaunch = ntiles + max_split;
     return ICM_OK;
 }
 
@@ -752,7 +763,8 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     R.strays = c->d_strays;
     R.ind_y = p->indenter_y;
     R.cost = c->fz.cost;
-    if ((rc = tile_order(c, ntiles, R.order))) return rc;
+    int nlaunch = ntiles;
+    if ((rc = tile_order(c, ntiles, R.order, nlaunch))) return rc;
     if ((rc = ensure_tmaps(c, P))) return rc;
     R.tmap = c->tmap_ok ? c->d_tmap : nullptr;
 
@@ -778,7 +790,7 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
         }
         int r;
         if (c->form == ICM_FORM_FP64) {
-            r = launch_variant<Pol64>(c, mode, ntiles, P, K64, c->fz.p64, R);
+            r = launch_variant<Pol64>(c, mode, nlaunch, P, K64, c->fz.p64, R);
         } else {
             Consts32 K = K32;
             if (c->d_harvest && harvest_now) {
@@ -786,8 +798,8 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
                 K.harvest_n = c->d_harvest_n;
                 K.harvest_cap = c->harvest_cap;
             }
-            r = (c->form == ICM_FORM_FP32_SURROGATE) ? launch_variant<Pol32S>(c, mode, ntiles, P, K, c->fz.p32, R)
-                                                     : launch_variant<Pol32>(c, mode, ntiles, P, K, c->fz.p32, R);
+            r = (c->form == ICM_FORM_FP32_SURROGATE) ? launch_variant<Pol32S>(c, mode, nlaunch, P, K, c->fz.p32, R)
+                                                     : launch_variant<Pol32>(c, mode, nlaunch, P, K, c->fz.p32, R);
         }
         if (e1) ICM_CUDA(cudaEventRecord(e1, c->stream));
         return r;
@@ -816,7 +828,7 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
         if (k < n && c->rebin_interval > 0 && k % c->rebin_interval == 0) {
             if ((rc = rebin_internal(c, P, c->internal_pq || any_pq))) return rc;
             R.group_base = c->bin.group_base;
-            if ((rc = tile_order(c, ntiles, R.order))) return rc;
+            if ((rc = tile_order(c, ntiles, R.order, nlaunch))) return rc;
         }
     }
     p->SimulationStep += n;
@@ -946,6 +958,15 @@ extern "C" int icm_set_rebin_interval(icm_ctx *c, int substeps)
     if (!c) return icm::fail(ICM_ERR_ARG, "null context");
     if (substeps < 0) return icm::fail(ICM_ERR_ARG, "re-binning interval must be >= 0");
     c->rebin_interval = substeps;
+    return ICM_OK;
+}
+
+extern "C" int icm_set_tile_split(icm_ctx *c, int max_tiles, double ratio)
+{
+    if (!c) return icm::fail(ICM_ERR_ARG, "null context");
+    if (max_tiles < 0 || !(ratio >= 0)) return icm::fail(ICM_ERR_ARG, "icm_set_tile_split: max_tiles >= 0, ratio >= 0");
+    c->split_max = max_tiles;
+    c->split_ratio = ratio;
     return ICM_OK;
 }
 
@@ -1675,7 +1696,7 @@ extern "C" int icm_ensemble_run(icm_ensemble *e, icy_SimParams *const *p, int n)
         ICM_CUDA(cudaMemsetAsync(c->d_hist, 0, sizeof(double) * 2 * (size_t)n, c->stream));
         c->hist_n = n;
         if (c->fz.cost_variant != c->tile_variant || c->fz.cost_ntiles != ntiles) {
-            ICM_CUDA(cudaMemsetAsync(c->fz.cost, 0, sizeof(unsigned) * (size_t)ntiles, c->stream));
+            ICM_CUDA(cudaMemsetAsync(c->fz.cost, 0, 2 * sizeof(unsigned) * (size_t)ntiles, c->stream));
             c->fz.cost_variant = c->tile_variant;
             c->fz.cost_ntiles = ntiles;
         }

@@ -106,6 +106,9 @@ struct TmapSet {
 // 2 an ensemble case scattered outside its active tiles, 4 a tensor copy of
 // a node region did not complete in time
 constexpr int kErrTmaTimeout = 4;
+
+// launch-order entries of the fused kernel (k_tile_order)
+constexpr int kTileMask = (1 << 29) - 1, kSplitBit = 1 << 29, kHalfBit = 1 << 30;
 constexpr int kTmaPolls = 1 << 22;
 
 // Copies the (RX x RY)-node region at node (rx0, ry0) of one grid buffer
@@ -691,7 +694,7 @@ __host__ __device__ constexpr size_t tile_dyn_bytes(int RN, int nwarps)
 template <class Pol, int TX, int TY, int MODE>
 __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename Pol::Consts &K,
                                           const typename Pol::Parts &A, const TileRun &R, const int t,
-                                          const CUtensorMap *tmaps, const bool tmaps_in_global)
+                                          const CUtensorMap *tmaps, const bool tmaps_in_global, const int part)
 {
     using real = typename Pol::real;
     using V2 = typename Pol::V2;
@@ -732,7 +735,13 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
 
     // 1. zero this tile in the buffer the next substep will scatter into;
     //    the flag is cleared only after every thread has read it
-    const bool zero_c = (MODE == kModeFull) && R.dirty[R.bufC][t];
+    // part 0: the whole tile; parts 1 and 2: the first and second half of
+    // the tile's cell groups (a heavy tile split over two CTAs). Both halves
+    // update the node region; the first owns the tile's zeroing and its
+    // reaction force.
+    const int NGT_ = TX * TY / 32;
+    const int g_lo = part == 2 ? NGT_ / 2 : 0, g_hi = part == 1 ? NGT_ / 2 : NGT_;
+    const bool zero_c = (MODE == kModeFull) && part != 2 && R.dirty[R.bufC][t];
     if (zero_c) {
         Node *gC = (Node *)R.grid[R.bufC];
         for (int k = tid; k < TX * TY; k += nthr) {
@@ -792,7 +801,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                         double f0 = 0, f1 = 0;
                         int bin;
                         Pol::node_velocity(P, K, nd[b], gx, gy, R.ind_x, R.ind_y, v0, v1, f0, f1, bin, contact_possible);
-                        bool own = gx >= x0 && gx < x0 + TX && gy >= y0 && gy < y0 + TY;
+                        bool own = part != 2 && gx >= x0 && gx < x0 + TX && gy >= y0 && gy < y0 + TY;
                         if (bin >= 0 && own) {
                             atomicAdd(&s_bins[2 * bin], f0);
                             atomicAdd(&s_bins[2 * bin + 1], f1);
@@ -862,7 +871,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
 
     // this warp's groups g = warp, warp + nwarps, ... (at most kMaxGroupsPerWarp)
     int ng_w = 0;
-    for (int g = warp; g < NGT; g += nwarps, ng_w++) {
+    for (int g = g_lo + warp; g < g_hi; g += nwarps, ng_w++) {
         const int c = t * CELLS + g * 32 + lane;
         const int cnt = R.cell_start[c + 1] - R.cell_start[c];
         s_wcnt[warp][ng_w][lane] = cnt;
@@ -897,7 +906,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         next_item(k, r, nk, nr);
         issue(nk, nr, cur ^ 1);
         __pipeline_wait_prior(1);
-        const int g = warp + k * nwarps;
+        const int g = g_lo + warp + k * nwarps;
         const int cl = g * 32 + lane;
         const int clx = cl % TX, cly = cl / TX;
         const int cbx = x0 + clx, cby = y0 + cly;  // the cell's base node
@@ -1166,14 +1175,28 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep(const __g
     // next one launch (its CTAs take free slots and wait here in turn)
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    const int t = R.order ? R.order[blockIdx.x] : blockIdx.x;
+    const int ntiles = R.ntx * R.nty;
+    // order entries: tile | split << 29 | second half << 30, or -1 (nothing)
+    int code;
+    if (R.order) {
+        code = R.order[blockIdx.x];
+    } else {
+        code = (int)blockIdx.x < ntiles ? (int)blockIdx.x : -1;
+    }
+    if (code < 0) return;
+    const int t = code & kTileMask;
+    const int part = (code & kSplitBit) ? ((code & kHalfBit) ? 2 : 1) : 0;
     if (MODE == kModeFull && threadIdx.x == 0) s_clock = clock64();
-    tile_body<Pol, TX, TY, MODE>(P, K, A, R, t, R.tmap ? T.m : nullptr, false);
+    tile_body<Pol, TX, TY, MODE>(P, K, A, R, t, R.tmap ? T.m : nullptr, false, part);
     if (MODE == kModeFull && R.cost) {
         __syncthreads();
         if (threadIdx.x == 0) {
+            // cost[t] and cost[ntiles + t]: the tile's two halves (the second
+            // is zero for a tile run whole)
             const long long dc = clock64() - s_clock;
-            R.cost[t] = (unsigned)(dc < 0 ? 0 : (dc > 0xffffffffll ? 0xffffffffll : dc));
+            const unsigned c = (unsigned)(dc < 0 ? 0 : (dc > 0xffffffffll ? 0xffffffffll : dc));
+            R.cost[part == 2 ? ntiles + t : t] = c;
+            if (part == 0) R.cost[ntiles + t] = 0;
         }
     }
 }
@@ -1252,12 +1275,13 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const
         }
     }
     __syncthreads();
-    tile_body<Pol, TX, TY, MODE>(sc.P, sc.K, sc.A, sc.R, t, sc.R.tmap, true);
+    tile_body<Pol, TX, TY, MODE>(sc.P, sc.K, sc.A, sc.R, t, sc.R.tmap, true, 0);
     if (MODE == kModeFull && sc.R.cost) {
         __syncthreads();
         if (threadIdx.x == 0) {
             const long long dc = clock64() - s_clock;
             sc.R.cost[t] = (unsigned)(dc < 0 ? 0 : (dc > 0xffffffffll ? 0xffffffffll : dc));
+            sc.R.cost[sc.ntiles + t] = 0;  // (the second-half slot of a single run's split)
         }
     }
 }
@@ -1278,16 +1302,44 @@ template <class Pol> __global__ void k_ens_check(const EnsCase<Pol> *__restrict_
 
 // Tile order by descending cost (ties by tile index): a bitonic sort of
 // (cost << 32 | ~tile) keys in shared memory, one CTA, n <= kMaxOrderTiles.
+// A tile's cost is cost[t] + cost[n + t] (its halves when it ran split).
+// The heaviest tiles whose cost exceeds ratio times the mean over tiles
+// holding particles, at most max_split of them, are split: their two halves
+// lead the order (two CTAs each), then the other tiles; the order has
+// n + max_split entries, the unused ones -1.
 constexpr int kMaxOrderTiles = 8192;
 constexpr int kOrderThreads = 1024;
 
-__global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsigned *cost, int *order)
+__global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsigned *cost, const int *tile_start,
+                                                              int max_split, float ratio, int *order)
 {
     extern __shared__ unsigned long long s_key[];
+    __shared__ unsigned long long s_sum;
+    __shared__ int s_busy, s_nsplit;
     int m = 1;
     while (m < n) m <<= 1;
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        s_key[i] = (i < n) ? (((unsigned long long)cost[i] << 32) | (0xffffffffu - (unsigned)i)) : 0ull;
+    if (threadIdx.x == 0) {
+        s_sum = 0;
+        s_busy = 0;
+        s_nsplit = 0;
+    }
+    __syncthreads();
+    unsigned long long sum = 0;
+    int busy = 0;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        unsigned c = 0;
+        if (i < n) {
+            const unsigned long long cc = (unsigned long long)cost[i] + cost[n + i];
+            c = cc > 0xffffffffull ? 0xffffffffu : (unsigned)cc;
+            if (tile_start[i + 1] > tile_start[i]) {
+                sum += c;
+                busy++;
+            }
+        }
+        s_key[i] = (i < n) ? (((unsigned long long)c << 32) | (0xffffffffu - (unsigned)i)) : 0ull;
+    }
+    atomicAdd(&s_sum, sum);
+    atomicAdd(&s_busy, busy);
     __syncthreads();
     for (int k = 2; k <= m; k <<= 1)
         for (int j = k >> 1; j > 0; j >>= 1) {
@@ -1304,7 +1356,23 @@ __global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsig
             }
             __syncthreads();
         }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) order[i] = (int)(0xffffffffu - (unsigned)(s_key[i] & 0xffffffffu));
+    // the split tiles are a prefix of the sorted list
+    const double thr = s_busy > 0 ? (double)ratio * (double)s_sum / (double)s_busy : 1e300;
+    const int lim = min(max_split, n);
+    for (int i = threadIdx.x; i < lim; i += blockDim.x)
+        if ((double)(s_key[i] >> 32) > thr && (i + 1 == lim || (double)(s_key[i + 1] >> 32) <= thr))
+            s_nsplit = i + 1;
+    __syncthreads();
+    const int S = s_nsplit;
+    for (int i = threadIdx.x; i < n + max_split; i += blockDim.x) {
+        int v = -1;
+        if (i < 2 * S) {
+            v = (int)(0xffffffffu - (unsigned)(s_key[i >> 1] & 0xffffffffu)) | kSplitBit | ((i & 1) ? kHalfBit : 0);
+        } else if (i < n + S) {
+            v = (int)(0xffffffffu - (unsigned)(s_key[i - S] & 0xffffffffu));
+        }
+        order[i] = v;
+    }
 }
 
 // ------------------------------------------------ binning, pack and unpack

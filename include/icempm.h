@@ -112,6 +112,13 @@ int icm_get_tile(icm_ctx *ctx, int *tile_variant, int *threads);
  * default 200). Particles that left their binned cell take a slower scatter
  * path until then. */
 int icm_set_rebin_interval(icm_ctx *ctx, int substeps);
+/* Fused forms: a tile whose last measured cost exceeds `ratio` times the
+ * mean over tiles holding particles runs as two CTAs (each half of its cell
+ * groups), at most `max_tiles` tiles per launch; the heaviest tiles -- the
+ * crushed zone at the indenter -- otherwise set the length of a launch late
+ * in a frame. Default 128 tiles, ratio 1.3; max_tiles 0 turns it off. No
+ * counterpart in the reference. */
+int icm_set_tile_split(icm_ctx *ctx, int max_tiles, double ratio);
 /* GPU_Implementation5::cuda_allocate_arrays (gpu_implementation5.cu:481-513):
  * device particle SoA, grid and force bins. Writes the device pointers and
  * pitches into *p and resets the error code. */

@@ -214,6 +214,31 @@ def test_model_step_runs_one_frame():
 
 
 @pytest.mark.parametrize("form", [im.FORM_FP64, im.FORM_FP32])
+def test_split_tiles_keep_parity(form):
+    """Every tile with a measured cost run as two CTAs (one per half of its
+    cell groups) from the first re-binning on: results match the oracle as
+    without splitting, reaction force included (only the first half adds
+    it)."""
+    p, soa = perturbed_case(seed=14)
+    n = 12
+    m = gpu_model(p, soa, form, 1, 128)
+    m.gpu.set_rebin_interval(3)
+    m.gpu.set_tile_split(4096, 0.0)
+    m.gpu.run_substeps(m.prms, n)
+    got = gpu_state(m)
+    q, ref, bins, err, hist = oracle_run(p, soa, n)
+    e = compare_states(p, got, ref, soa)
+    if form == im.FORM_FP64:
+        assert e["crushed_mismatch"] == 0 and max(e["disp_rel"], e["vel"], e["strain"], e["Bp"]) < FP64_TOL, e
+        assert max_rel(m.gpu.force_history(n), hist) < FP64_TOL
+    else:
+        assert e["disp_h"] < 1e-4 and e["vel"] < 5e-3, e
+        assert max_rel(m.gpu.force_history(n), hist) < 1e-2
+    assert e["grain_mismatch"] == 0
+    assert m.gpu.error_code == 0
+
+
+@pytest.mark.parametrize("form", [im.FORM_FP64, im.FORM_FP32])
 def test_rebinning_keeps_parity(form):
     """Re-binning the particles between substeps changes only their order:
     results match the oracle as without it."""
