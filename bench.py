@@ -18,6 +18,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import gc
 import json
 import os
 import subprocess
@@ -691,8 +692,12 @@ def ensemble_section(args, device, flush):
         return ms
 
     def close(ms):
+        # every release happens here, before the next arm's timed runs
         for m in ms:
             m.gpu.close()
+        ms.clear()
+        gc.collect()
+        torch.cuda.synchronize()
 
     def ev():
         return torch.cuda.Event(enable_timing=True)

@@ -306,8 +306,8 @@ static int ensure_slots(icm_ctx *c, int form, size_t nslots)
     dfree(c->bin.pid);
     free_spare(c);
     // the same headroom as the spare set: re-binning swaps the two sets, and
-    // the slot count drifts a little with every re-binning
-    nslots += nslots / 4 + 4096;
+    // the slot count grows as crushing packs more particles into fewer cells
+    nslots += nslots / 2 + 4096;
     c->fz.form = form;
     c->fz.cap_pts = nslots;
     c->bin.cap_slots = nslots;
@@ -501,10 +501,10 @@ static int ensure_spare(icm_ctx *c, size_t nslots)
 {
     if (c->fz.spare_cap >= nslots) return ICM_OK;
     free_spare(c);
-    // headroom: the slot count changes a little at every re-binning, and a
-    // reallocation (cudaFree synchronises the device) costs far more than
-    // the memory
-    nslots += nslots / 4 + 4096;
+    // headroom: the slot count changes at every re-binning (it grows as
+    // crushing packs more particles into fewer cells), and a reallocation
+    // (cudaFree synchronises the device) costs far more than the memory
+    nslots += nslots / 2 + 4096;
     int rc;
     if ((rc = dalloc(&c->fz.spare_pid, nslots)) || (rc = dalloc(&c->fz.slot_key, nslots))) return rc;
     if (c->fz.form == ICM_FORM_FP64) {
