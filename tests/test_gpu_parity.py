@@ -214,14 +214,15 @@ def test_model_step_runs_one_frame():
 
 
 @pytest.mark.parametrize("form", [im.FORM_FP64, im.FORM_FP32])
-def test_split_tiles_keep_parity(form):
+@pytest.mark.parametrize("tile", [0, 1, 3])
+def test_split_tiles_keep_parity(form, tile):
     """Every tile with a measured cost run as two CTAs (one per half of its
     cell groups) from the first re-binning on: results match the oracle as
     without splitting, reaction force included (only the first half adds
     it)."""
     p, soa = perturbed_case(seed=14)
     n = 12
-    m = gpu_model(p, soa, form, 1, 128)
+    m = gpu_model(p, soa, form, tile, 128)
     m.gpu.set_rebin_interval(3)
     m.gpu.set_tile_split(4096, 0.0)
     m.gpu.run_substeps(m.prms, n)
