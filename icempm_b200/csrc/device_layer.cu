@@ -1269,6 +1269,11 @@ struct icm_ensemble {
     std::vector<cudaEvent_t> events;  // one per case, plus one for the ensemble stream
     unsigned char *h_stage = nullptr;  // pinned: every case's tile starts, costs and dirty flags
     size_t stage_cap = 0;
+    // heavy tiles split over two CTAs, as icm_set_tile_split; off by default:
+    // the launch list of many cases has work enough that no single tile sets
+    // its length (64 cases: 0.520 ms per substep without, 0.528 with)
+    int split_max = 0;
+    double split_ratio = 1.3;
 };
 
 namespace {
@@ -1439,7 +1444,7 @@ int ens_active_tiles(icm_ensemble *e, const std::vector<icy_SimParams> &P)
     std::vector<TileGeom> geo(nc);
     for (size_t i = 0; i < nc; i++) {
         geometry(P[i], e->variant, geo[i], nt[i]);
-        off[i + 1] = off[i] + 4 * ((size_t)nt[i] + 1) + 4 * (size_t)nt[i] + ((3 * (size_t)nt[i] + 3) & ~(size_t)3);
+        off[i + 1] = off[i] + 4 * ((size_t)nt[i] + 1) + 8 * (size_t)nt[i] + ((3 * (size_t)nt[i] + 3) & ~(size_t)3);
     }
     if (off[nc] > e->stage_cap) {
         if (e->h_stage) cudaFreeHost(e->h_stage);
@@ -1456,20 +1461,22 @@ int ens_active_tiles(icm_ensemble *e, const std::vector<icy_SimParams> &P)
         unsigned char *b = e->h_stage + off[i];
         const size_t n = (size_t)nt[i];
         ICM_CUDA(cudaMemcpyAsync(b, c->bin.tile_start, 4 * (n + 1), cudaMemcpyDeviceToHost, e->stream));
-        ICM_CUDA(cudaMemcpyAsync(b + 4 * (n + 1), c->fz.cost, 4 * n, cudaMemcpyDeviceToHost, e->stream));
-        ICM_CUDA(cudaMemcpyAsync(b + 8 * n + 4, c->fz.dirty, 3 * n, cudaMemcpyDeviceToHost, e->stream));
+        ICM_CUDA(cudaMemcpyAsync(b + 4 * (n + 1), c->fz.cost, 8 * n, cudaMemcpyDeviceToHost, e->stream));
+        ICM_CUDA(cudaMemcpyAsync(b + 12 * n + 4, c->fz.dirty, 3 * n, cudaMemcpyDeviceToHost, e->stream));
     }
     ICM_CUDA(cudaStreamSynchronize(e->stream));
     std::vector<Item> items;
     std::vector<uint8_t> mask;
+    unsigned long long busy_sum = 0;
+    long long nbusy = 0;
     e->active_off.assign(nc, 0);
     for (size_t i = 0; i < nc; i++) {
         const int ntiles = nt[i];
         const TileGeom &g = geo[i];
         const unsigned char *b = e->h_stage + off[i];
         const int *ts = reinterpret_cast<const int *>(b);
-        const unsigned *cost = reinterpret_cast<const unsigned *>(b + 4 * ((size_t)ntiles + 1));
-        const uint8_t *dirty = b + 8 * (size_t)ntiles + 4;
+        const unsigned *cost = reinterpret_cast<const unsigned *>(b + 4 * ((size_t)ntiles + 1));  // two halves
+        const uint8_t *dirty = b + 12 * (size_t)ntiles + 4;
         e->active_off[i] = mask.size();
         mask.resize(mask.size() + (size_t)ntiles, 0);
         uint8_t *busy = mask.data() + e->active_off[i];
@@ -1484,9 +1491,32 @@ int ens_active_tiles(icm_ensemble *e, const std::vector<icy_SimParams> &P)
                 }
         }
         for (int t = 0; t < ntiles; t++)
-            if (busy[t]) items.push_back({cost[t], (int)i, t});
+            if (busy[t]) {
+                const unsigned long long cc = (unsigned long long)cost[t] + cost[(size_t)ntiles + t];
+                items.push_back({cc > 0xffffffffull ? 0xffffffffu : (unsigned)cc, (int)i, t});
+                if (ts[t + 1] > ts[t]) {
+                    busy_sum += cc;
+                    nbusy++;
+                }
+            }
     }
+    // the heaviest tiles (cost above split_ratio times the mean over tiles
+    // with particles, at most split_max) run as two CTAs, as in single runs
     std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) { return a.cost > b.cost; });
+    if (nbusy > 0 && e->split_max > 0) {
+        const double thr = e->split_ratio * (double)busy_sum / (double)nbusy;
+        const size_t lim = std::min(items.size(), (size_t)e->split_max);
+        size_t S = 0;
+        while (S < lim && (double)items[S].cost > thr) S++;
+        std::vector<Item> second(S);
+        for (size_t k = 0; k < S; k++) {
+            items[k].cost /= 2;
+            items[k].t |= kSplitBit;
+            second[k] = {items[k].cost, items[k].c, items[k].t | kHalfBit};
+        }
+        items.insert(items.end(), second.begin(), second.end());
+        std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) { return a.cost > b.cost; });
+    }
     std::vector<int> tc(items.size()), tl(items.size());
     for (size_t k = 0; k < items.size(); k++) {
         tc[k] = items[k].c;
@@ -1658,6 +1688,14 @@ extern "C" int icm_ensemble_set(icm_ensemble *e, int rebin_interval, int use_gra
     if (!e || rebin_interval < 0) return icm::fail(ICM_ERR_ARG, "icm_ensemble_set: bad argument");
     e->rebin_interval = rebin_interval;
     e->graphs = use_graphs != 0;
+    return ICM_OK;
+}
+
+extern "C" int icm_ensemble_set_split(icm_ensemble *e, int max_tiles, double ratio)
+{
+    if (!e || max_tiles < 0 || !(ratio >= 0)) return icm::fail(ICM_ERR_ARG, "icm_ensemble_set_split: bad argument");
+    e->split_max = max_tiles;
+    e->split_ratio = ratio;
     return ICM_OK;
 }
 

@@ -1248,7 +1248,10 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if ((int)blockIdx.x >= *L.nactive) return;
-    const int c = L.tile_case[blockIdx.x], t = L.tile_local[blockIdx.x];
+    // tile_local: tile | split << 29 | second half << 30 (as the single-run order)
+    const int c = L.tile_case[blockIdx.x], code = L.tile_local[blockIdx.x];
+    const int t = code & kTileMask;
+    const int part = (code & kSplitBit) ? ((code & kHalfBit) ? 2 : 1) : 0;
     {
         const uint32_t *src = reinterpret_cast<const uint32_t *>(cases + c);
         uint32_t *dst = reinterpret_cast<uint32_t *>(&sc);
@@ -1275,13 +1278,14 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const
         }
     }
     __syncthreads();
-    tile_body<Pol, TX, TY, MODE>(sc.P, sc.K, sc.A, sc.R, t, sc.R.tmap, true, 0);
+    tile_body<Pol, TX, TY, MODE>(sc.P, sc.K, sc.A, sc.R, t, sc.R.tmap, true, part);
     if (MODE == kModeFull && sc.R.cost) {
         __syncthreads();
         if (threadIdx.x == 0) {
             const long long dc = clock64() - s_clock;
-            sc.R.cost[t] = (unsigned)(dc < 0 ? 0 : (dc > 0xffffffffll ? 0xffffffffll : dc));
-            sc.R.cost[sc.ntiles + t] = 0;  // (the second-half slot of a single run's split)
+            const unsigned cc = (unsigned)(dc < 0 ? 0 : (dc > 0xffffffffll ? 0xffffffffll : dc));
+            sc.R.cost[part == 2 ? sc.ntiles + t : t] = cc;
+            if (part == 0) sc.R.cost[sc.ntiles + t] = 0;
         }
     }
 }

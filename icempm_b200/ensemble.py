@@ -20,6 +20,7 @@ def _sigs():
         ("icm_ensemble_add", i, [vp, vp]),
         ("icm_ensemble_size", i, [vp]),
         ("icm_ensemble_set", i, [vp, i, i]),
+        ("icm_ensemble_set_split", i, [vp, i, C.c_double]),
         ("icm_ensemble_run", i, [vp, C.POINTER(C.POINTER(SimParams)), i]),
         ("icm_ensemble_stream", vp, [vp]),
     ):
@@ -48,6 +49,10 @@ class Ensemble:
 
     def set(self, rebin_interval: int = 200, graphs: bool = True) -> None:
         _check(_sigs().icm_ensemble_set(self._e, rebin_interval, 1 if graphs else 0))
+
+    def set_split(self, max_tiles: int = 128, ratio: float = 1.3) -> None:
+        """Heavy tiles run as two CTAs (max_tiles 0, the default: off)."""
+        _check(_sigs().icm_ensemble_set_split(self._e, max_tiles, ratio))
 
     def run(self, n: int) -> None:
         arr = (C.POINTER(SimParams) * len(self.models))(*[C.pointer(m.prms) for m in self.models])

@@ -283,6 +283,11 @@ int icm_ensemble_set(icm_ensemble *e, int rebin_interval, int use_graphs);
  * re-binnings (mass that no launch consumed; a shorter re-binning interval
  * avoids it) gets bit 2 set in its error word (icm_transfer_from_device). */
 int icm_ensemble_run(icm_ensemble *e, icy_SimParams *const *p, int n);
+/* Heavy tiles of the launch list run as two CTAs, as icm_set_tile_split
+ * (ratio to the mean over tiles with particles, across all cases). Default
+ * off (max_tiles 0): a list of many cases has work enough that no single
+ * tile sets the length of a launch. */
+int icm_ensemble_set_split(icm_ensemble *e, int max_tiles, double ratio);
 /* The ensemble's CUDA stream (cudaStream_t). */
 void *icm_ensemble_stream(icm_ensemble *e);
 

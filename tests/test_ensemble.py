@@ -66,6 +66,36 @@ def test_ensemble_matches_cases_run_alone(form, graphs):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("form", [im.FORM_FP64, im.FORM_FP32])
+def test_ensemble_split_tiles_match_cases_run_alone(form):
+    """Every measured tile of every case split over two CTAs from the first
+    re-binning on: each case still ends where it ends alone."""
+    n, rebin = 13, 4
+    cases = [_case(*c) for c in CASES]
+    ens = Ensemble(form, tile=1, threads=128)
+    ens.set(rebin_interval=rebin)
+    ens.set_split(4096, 0.0)
+    models = []
+    for p, soa in cases:
+        m = gpu_model(p, soa, form, tile=1, threads=128)
+        ens.add(m)
+        models.append(m)
+    ens.run(n)
+    tol_pos, tol = (1e-9, 1e-9) if form == im.FORM_FP64 else (1e-5, 1e-4)
+    for (p, soa), m in zip(cases, models):
+        got, hist = gpu_state(m), m.gpu.force_history(n)
+        _, ref, href = _alone(p, soa, form, n, rebin)
+        err = compare_states(p, got, ref, soa)
+        assert err["disp_h"] <= tol_pos and err["strain"] <= tol and err["vel"] <= tol, err
+        scale = max(np.abs(href).max(), 1e-30)
+        assert np.abs(hist - href).max() <= 1e3 * tol * scale
+        assert m.gpu.error_code == 0
+    ens.close()
+    for m in models:
+        m.gpu.close()
+
+
+@pytest.mark.gpu
 def test_ensemble_runs_compose():
     """Two ensemble runs continue each other (a second run re-packs nothing
     and reuses its captured graph)."""
