@@ -199,6 +199,30 @@ static Consts32 make_consts32(const icy_SimParams &P)
     k.four_h_inv = (float)(4.0 * P.cellsize_inv);
     k.dt_g = (float)(P.InitialTimeStep * P.Gravity);
     k.vmax = (float)(0.5 * P.cellsize / P.InitialTimeStep);
+    // The box p in (-1 MPa, pmax_min / 2), q^2 < inside_q2 lies inside the
+    // failure surface of every grain with residues r1 in 0..20, r2 in 0..29,
+    // r3 in 0..10 (ids >= 0), by a factor of at least 4 in the terms that
+    // failure_side32 compares: with a = pmax, b = -pmin, both surface
+    // branches allow q^2 >= (16/9) qmax^2 ab/(a+b)^2 there, and ab/(a+b)^2
+    // takes its minimum over the box of (a, b) at a corner.
+    {
+        const double gv = P.GrainVariability, ics = P.IceCompressiveStrength * 1e-6,
+                     its = P.IceTensileStrength * 1e-6, iss = P.IceShearStrength * 1e-6;
+        const double a_lo = ics * (1 + gv * 0.05 * -10), a_hi = ics * (1 + gv * 0.05 * 10);
+        const double b_lo = its * (1 + gv * 0.033 * -15), b_hi = its * (1 + gv * 0.033 * 14);
+        const double q_lo = iss * (1 + gv * 0.1 * -10);
+        k.inside_plo = -1.0f;
+        k.inside_phi = 0.0f;
+        k.inside_q2 = 0.0f;
+        if (a_lo > 2.0 && b_lo > 0 && q_lo > 0 && a_hi > 0 && b_hi > 0) {
+            double g = 1e300;
+            const double as[2] = {a_lo, a_hi}, bs[2] = {b_lo, b_hi};
+            for (double a : as)
+                for (double b : bs) g = std::min(g, a * b / ((a + b) * (a + b)));
+            k.inside_phi = (float)(0.5 * a_lo);
+            k.inside_q2 = (float)(0.25 * (16.0 / 9.0) * q_lo * q_lo * g);
+        }
+    }
     return k;
 }
 

@@ -41,6 +41,10 @@ struct Consts32 {
     float gv, ics, its, iss;                        // grain variability, strengths in MPa
     float four_h_inv;
     float dt_g, vmax;                               // dt*gravity, 0.5 h/dt
+    // a box in (p, q) (MPa) inside every failure surface that a grain with a
+    // non-negative id can have, with a wide margin: a particle of such a
+    // grain inside it needs no table lookup to be found intact (q2 = 0: none)
+    float inside_plo, inside_phi, inside_q2;
     // trial states of crushed particles (H, Jp_inv, meta: 6 words each) are
     // appended here while harvest is set (training data of the surrogate)
     float *harvest;
@@ -155,7 +159,11 @@ __device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTabl
     if (!(v.J > 0.25f) || meta32_crushed(meta)) return kC32_NEEDS_FP64;
     float p = -0.5f * v.s2;
     float q = 2.0f * v.s1 * approx_sqrt(v.hd * v.hd + v.b01 * v.b01);
-    if (failure_side32(T, meta, p, q) != 0) return kC32_NEEDS_FP64;
+    // residues at or above their offsets: the grain id is not negative
+    const bool grain_nonneg = (meta & 63u) >= 20u && ((meta >> 6) & 63u) >= 29u && ((meta >> 12) & 31u) >= 10u;
+    const float pm = p * 1e-6f, qm = q * 1e-6f;
+    const bool clearly_inside = grain_nonneg && pm > k.inside_plo && pm < k.inside_phi && qm * qm < k.inside_q2;
+    if (!clearly_inside && failure_side32(T, meta, p, q) != 0) return kC32_NEEDS_FP64;
     p_tr = p;
     q_tr = q;
     tau = tau32(v);
