@@ -1367,8 +1367,9 @@ int ens_launch_variant(icm_ensemble *e, int mode, int grid, const void *d_cases,
 int ens_launch(icm_ensemble *e, int mode, int grid, int j)
 {
     EnsLaunch L{e->d_seg_base, j, e->d_tile_case, e->d_tile_local, e->d_nactive};
-    return e->form == ICM_FORM_FP64 ? ens_launch_variant<Pol64>(e, mode, grid, e->d_cases, L)
-                                    : ens_launch_variant<Pol32>(e, mode, grid, e->d_cases, L);
+    if (e->form == ICM_FORM_FP64) return ens_launch_variant<Pol64>(e, mode, grid, e->d_cases, L);
+    if (e->form == ICM_FORM_FP32_SURROGATE) return ens_launch_variant<Pol32S>(e, mode, grid, e->d_cases, L);
+    return ens_launch_variant<Pol32>(e, mode, grid, e->d_cases, L);
 }
 
 // e->stream waits for the cases' streams (to = true) or they for it
@@ -1408,6 +1409,12 @@ int ens_upload_cases(icm_ensemble *e, const std::vector<icy_SimParams> &P, icy_S
                 d.K.harvest_n = c->d_harvest_n;
                 d.K.harvest_cap = c->harvest_cap;
                 d.harvest_every = c->harvest_every;
+            }
+            if constexpr (std::is_same<Pol, Pol32S>::value) {
+                // each case its own network, tolerance and counters
+                d.K.mlp = c->d_mlp;
+                d.K.mlp_tol = c->mlp_tol;
+                d.K.mlp_counts = c->d_mlp_counts;
             }
         }
         TileGeom g;
@@ -1575,7 +1582,9 @@ int ens_upload(icm_ensemble *e, const std::vector<icy_SimParams> &P, icy_SimPara
 {
     const int rc = ens_active_tiles(e, P);
     if (rc) return rc;
-    return e->form == ICM_FORM_FP64 ? ens_upload_cases<Pol64>(e, P, p, n) : ens_upload_cases<Pol32>(e, P, p, n);
+    if (e->form == ICM_FORM_FP64) return ens_upload_cases<Pol64>(e, P, p, n);
+    if (e->form == ICM_FORM_FP32_SURROGATE) return ens_upload_cases<Pol32S>(e, P, p, n);
+    return ens_upload_cases<Pol32>(e, P, p, n);
 }
 
 int ens_check(icm_ensemble *e)
@@ -1583,6 +1592,8 @@ int ens_check(icm_ensemble *e)
     const int nc = (int)e->cases.size();
     if (e->form == ICM_FORM_FP64)
         k_ens_check<Pol64><<<nc, 128, 0, e->stream>>>(static_cast<const EnsCase<Pol64> *>(e->d_cases));
+    else if (e->form == ICM_FORM_FP32_SURROGATE)
+        k_ens_check<Pol32S><<<nc, 128, 0, e->stream>>>(static_cast<const EnsCase<Pol32S> *>(e->d_cases));
     else
         k_ens_check<Pol32><<<nc, 128, 0, e->stream>>>(static_cast<const EnsCase<Pol32> *>(e->d_cases));
     ICM_LAUNCHED("k_ens_check");
@@ -1635,8 +1646,10 @@ extern "C" int icm_ensemble_create(icm_ensemble **out, int device, int form, int
 {
     if (!out) return icm::fail(ICM_ERR_ARG, "icm_ensemble_create: null out");
     *out = nullptr;
-    if (form != ICM_FORM_FP32 && form != ICM_FORM_FP64)
-        return icm::fail(ICM_ERR_ARG, "icm_ensemble_create: the fused FP32 or FP64 form");
+    if (form != ICM_FORM_FP32 && form != ICM_FORM_FP64 && form != ICM_FORM_FP32_SURROGATE)
+        return icm::fail(ICM_ERR_ARG, "icm_ensemble_create: a fused form (FP32, FP64 or FP32 surrogate)");
+    if (form == ICM_FORM_FP32_SURROGATE && threads > 32 * Pol32S::kWarps)
+        return icm::fail(ICM_ERR_ARG, "icm_ensemble_create: surrogate form: at most 128 threads per block");
     if (tile_variant < 0 || tile_variant > 3 || threads < 32 || threads > 256 || threads % 32)
         return icm::fail(ICM_ERR_ARG, "icm_ensemble_create: tile variant 0..3, threads 32..256 in warps");
     int count = 0;
@@ -1743,6 +1756,8 @@ extern "C" int icm_ensemble_run(icm_ensemble *e, icy_SimParams *const *p, int n)
         if ((rc = check_params(c, p[i]))) return rc;
         if (c->form != e->form || c->tile_variant != e->variant || c->threads != e->threads)
             return icm::fail(ICM_ERR_STATE, "icm_ensemble_run: a case's form or tile was changed after icm_ensemble_add");
+        if (e->form == ICM_FORM_FP32_SURROGATE && !c->d_mlp)
+            return icm::fail(ICM_ERR_STATE, "icm_ensemble_run: surrogate form: a case without a network (icm_set_surrogate)");
         P[i] = kernel_params(c, p[i]);
         if (!c->internal_valid || c->fz.form != storage_form(c->form) || c->internal_variant != c->tile_variant) {
             if ((rc = ensure_ref(c)) || (rc = pack(c, P[i]))) return rc;

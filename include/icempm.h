@@ -266,8 +266,9 @@ int icm_harvest_pairs(icm_ctx *ctx, const icy_SimParams *p, float *x, float *y, 
  * order of float atomics: icm_force_history, icm_transfer_from_device etc.
  * read them from the case's context. */
 typedef struct icm_ensemble icm_ensemble;
-/* form: ICM_FORM_FP32 or ICM_FORM_FP64; tile_variant and threads as in
- * icm_set_tile. */
+/* form: ICM_FORM_FP32, ICM_FORM_FP64 or ICM_FORM_FP32_SURROGATE (each case
+ * with its own network from icm_set_surrogate; at most 128 threads);
+ * tile_variant and threads as in icm_set_tile. */
 int icm_ensemble_create(icm_ensemble **out, int device, int form, int tile_variant, int threads);
 int icm_ensemble_destroy(icm_ensemble *e);
 /* Adds a case (arrays allocated, points uploaded); sets its form and tile

@@ -121,6 +121,8 @@ def test_ensemble_argument_errors():
     with pytest.raises(RuntimeError):
         Ensemble(im.FORM_FP64_STEPWISE)
     with pytest.raises(RuntimeError):
+        Ensemble(im.FORM_FP32_SURROGATE, tile=1, threads=256)  # the surrogate form's 128-thread limit
+    with pytest.raises(RuntimeError):
         Ensemble(im.FORM_FP32, tile=3, threads=32)  # 32x16 tile needs 128 threads
 
 
@@ -215,6 +217,59 @@ def test_ensemble_harvest_matches_cases_run_alone():
         for col in range(3):
             u, v = np.sort(x[:, col])[:k], np.sort(xa[:, col])[:k]
             assert np.percentile(np.abs(u - v), 99) <= 1e-3
+    ens.close()
+    for m in models:
+        m.gpu.close()
+
+
+@pytest.mark.gpu
+def test_ensemble_surrogate_form_matches_cases_run_alone():
+    """The surrogate form inside an ensemble: each case carries its own
+    network, tolerance and counters; each ends close to the same case run
+    alone with the same network (accepted predictions may flip near the
+    tolerance when float atomics sum in another order)."""
+    from icempm_b200 import surrogate as sg
+
+    def crushing(seed):
+        p = params()
+        return p, scene(p, seed=seed, perturb=2e-3, vel=0.05, crushed_frac=0.5, jp_spread=0.005)
+
+    cases = [crushing(4), crushing(6)]
+    h = gpu_model(*cases[0], im.FORM_FP32, tile=1, threads=128)
+    sg.set_harvest(h.gpu, 200000, 1)
+    h.gpu.run_substeps(h.prms, 10)
+    x, y = sg.harvest_pairs(h.gpu, h.prms, 200000)
+    h.gpu.close()
+    net, _ = sg.fit(x, y, steps=800, batch_tiles=16, lr=3e-3, seed=1)
+
+    n, rebin, tol = 9, 4, 0.05
+    ens = Ensemble(im.FORM_FP32_SURROGATE, tile=1, threads=128)
+    ens.set(rebin_interval=rebin)
+    models = []
+    for p, soa in cases:
+        m = gpu_model(p, soa, im.FORM_FP32_SURROGATE, tile=1, threads=128)
+        sg.set_surrogate(m.gpu, net, tol)
+        ens.add(m)
+        models.append(m)
+    ens.run(n)
+    for (p, soa), m in zip(cases, models):
+        got = gpu_state(m)
+        acc, exact = sg.counts(m.gpu)
+        a = gpu_model(p, soa, im.FORM_FP32_SURROGATE, tile=1, threads=128)
+        sg.set_surrogate(a.gpu, net, tol)
+        a.gpu.set_rebin_interval(rebin)
+        a.gpu.run_substeps(a.prms, n)
+        ref = gpu_state(a)
+        acc_a, exact_a = sg.counts(a.gpu)
+        a.gpu.close()
+        assert acc > 0 and abs((acc + exact) - (acc_a + exact_a)) <= 0.02 * (acc_a + exact_a), (acc, exact, acc_a, exact_a)
+        err = compare_states(p, got, ref, soa)
+        G, R = im.SoA(got, p.nPtsPitch, p.nPts), im.SoA(ref, p.nPtsPitch, p.nPts)
+        eye = np.array([1.0, 0.0, 0.0, 1.0])[:, None]
+        per = np.abs(G.Fe - R.Fe).max(axis=0) / np.abs(R.Fe - eye).max()
+        assert err["disp_h"] <= 1e-3, err
+        assert np.percentile(per, 99) <= 2e-2, np.percentile(per, 99)
+        assert m.gpu.error_code == 0
     ens.close()
     for m in models:
         m.gpu.close()
