@@ -694,7 +694,8 @@ __host__ __device__ constexpr size_t tile_dyn_bytes(int RN, int nwarps)
 template <class Pol, int TX, int TY, int MODE>
 __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename Pol::Consts &K,
                                           const typename Pol::Parts &A, const TileRun &R, const int t,
-                                          const CUtensorMap *tmaps, const bool tmaps_in_global, const int part)
+                                          const CUtensorMap *tmaps, const bool tmaps_in_global, const int part,
+                                          const bool pdl_wait)
 {
     using real = typename Pol::real;
     using V2 = typename Pol::V2;
@@ -721,6 +722,42 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     const int tid = threadIdx.x, nthr = blockDim.x;
     Node *gA = (Node *)R.grid[R.bufA];
     Node *gB = (Node *)R.grid[R.bufB];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+    constexpr int CELLS = TX * TY;
+    // part 0: the whole tile; parts 1 and 2: the first and second half of
+    // the tile's cell groups (a heavy tile split over two CTAs). Both halves
+    // update the node region; the first owns the tile's zeroing and its
+    // reaction force.
+    const int NGT_ = TX * TY / 32;
+    const int g_lo = part == 2 ? NGT_ / 2 : 0, g_hi = part == 1 ? NGT_ / 2 : NGT_;
+    // What depends only on the binning (unchanged since the last re-binning
+    // or pack, both finished before this launch could start) is set up
+    // before the wait for the previous substep: this warp's groups g = warp,
+    // warp + nwarps, ... (at most kMaxGroupsPerWarp) with their cell counts,
+    // rounds and slot bases, and the grain tables.
+    int ng_w = 0;
+    if (p1 > p0) {
+        for (int g = g_lo + warp; g < g_hi; g += nwarps, ng_w++) {
+            const int c = t * CELLS + g * 32 + lane;
+            const int cnt = R.cell_start[c + 1] - R.cell_start[c];
+            s_wcnt[warp][ng_w][lane] = cnt;
+            const int rounds = __reduce_max_sync(FULL, cnt);
+            if (lane == 0) {
+                s_wrounds[warp][ng_w] = rounds;
+                s_wgbase[warp][ng_w] = R.group_base[(t * CELLS >> 5) + g];
+            }
+        }
+        __syncwarp();
+        if (MODE != kModeP2GOnly) Pol::init_tables(s_tab, K, tid, nthr);
+    }
+    // launched as a programmatic dependent: wait until the previous kernel
+    // of the stream has completed and its writes are visible, then let the
+    // next one launch (its CTAs take free slots, set up, and wait here)
+    if (pdl_wait) {
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    }
     // a full substep of a tile with particles stages its node region with
     // one tensor copy into the (not yet used) accumulation regions, issued
     // here so that it lands while the tile zeroes and sets up
@@ -735,12 +772,6 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
 
     // 1. zero this tile in the buffer the next substep will scatter into;
     //    the flag is cleared only after every thread has read it
-    // part 0: the whole tile; parts 1 and 2: the first and second half of
-    // the tile's cell groups (a heavy tile split over two CTAs). Both halves
-    // update the node region; the first owns the tile's zeroing and its
-    // reaction force.
-    const int NGT_ = TX * TY / 32;
-    const int g_lo = part == 2 ? NGT_ / 2 : 0, g_hi = part == 1 ? NGT_ / 2 : NGT_;
     const bool zero_c = (MODE == kModeFull) && part != 2 && R.dirty[R.bufC][t];
     if (zero_c) {
         Node *gC = (Node *)R.grid[R.bufC];
@@ -770,7 +801,6 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         }
     }
     if (tid < 9) s_mark[tid] = 0;
-    if (np > 0 && MODE != kModeP2GOnly) Pol::init_tables(s_tab, K, tid, nthr);
 
     // 2. grid update of the region (velocities into shared memory)
     if (MODE != kModeP2GOnly) {
@@ -858,30 +888,13 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     // reach the same node in different steps). A particle whose base node is
     // no longer its binned cell (it moved since binning) scatters on its
     // own: shared atomics inside the region, global atomics beyond it.
-    const unsigned FULL = 0xffffffffu;
-    const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
     const real h = Pol::h(P, K), m = Pol::mass(P, K), fhi = Pol::four_h_inv(P, K), sc = Pol::stress_c(P, K);
-    constexpr int CELLS = TX * TY;
-    constexpr int NGT = CELLS / 32;  // groups of 32 cells in the tile
     int bad = 0;
     unsigned redo_count = 0, stray_count = 0, mlp_ok = 0, mlp_fb = 0;
     Acc *wacc = s_acc + warp * RN;
     typename Pol::Stage *stage =
         reinterpret_cast<typename Pol::Stage *>(s_dyn + tile_region_bytes<Pol, MODE>(RN, nwarps)) + 2 * warp;
 
-    // this warp's groups g = warp, warp + nwarps, ... (at most kMaxGroupsPerWarp)
-    int ng_w = 0;
-    for (int g = g_lo + warp; g < g_hi; g += nwarps, ng_w++) {
-        const int c = t * CELLS + g * 32 + lane;
-        const int cnt = R.cell_start[c + 1] - R.cell_start[c];
-        s_wcnt[warp][ng_w][lane] = cnt;
-        const int rounds = __reduce_max_sync(FULL, cnt);
-        if (lane == 0) {
-            s_wrounds[warp][ng_w] = rounds;
-            s_wgbase[warp][ng_w] = R.group_base[(t * CELLS >> 5) + g];
-        }
-    }
-    __syncwarp();
     // work items (k, r): round r of the warp's k-th group; the next item's
     // particle state is copied into the other stage while this one computes
     auto next_item = [&](int k, int r, int &nk, int &nr) {
@@ -1170,11 +1183,6 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep(const __g
                                                       const __grid_constant__ TmapSet T)
 {
     __shared__ long long s_clock;
-    // launched as a programmatic dependent: wait until the previous kernel
-    // of the stream has completed and its writes are visible, then let the
-    // next one launch (its CTAs take free slots and wait here in turn)
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int ntiles = R.ntx * R.nty;
     // order entries: tile | split << 29 | second half << 30, or -1 (nothing)
     int code;
@@ -1187,7 +1195,7 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep(const __g
     const int t = code & kTileMask;
     const int part = (code & kSplitBit) ? ((code & kHalfBit) ? 2 : 1) : 0;
     if (MODE == kModeFull && threadIdx.x == 0) s_clock = clock64();
-    tile_body<Pol, TX, TY, MODE>(P, K, A, R, t, R.tmap ? T.m : nullptr, false, part);
+    tile_body<Pol, TX, TY, MODE>(P, K, A, R, t, R.tmap ? T.m : nullptr, false, part, true);
     if (MODE == kModeFull && R.cost) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1244,9 +1252,10 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const
 {
     __shared__ __align__(16) EnsCase<Pol> sc;
     __shared__ long long s_clock;
-    // programmatic dependent of the previous substep (see k_tile_substep)
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    // a programmatic dependent of the previous substep (see k_tile_substep):
+    // the launch list, the case descriptors and the segment's first substep
+    // index are written before the segment starts, so they are read before
+    // tile_body waits for the previous substep
     if ((int)blockIdx.x >= *L.nactive) return;
     // tile_local: tile | split << 29 | second half << 30 (as the single-run order)
     const int c = L.tile_case[blockIdx.x], code = L.tile_local[blockIdx.x];
@@ -1278,7 +1287,7 @@ __global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const
         }
     }
     __syncthreads();
-    tile_body<Pol, TX, TY, MODE>(sc.P, sc.K, sc.A, sc.R, t, sc.R.tmap, true, part);
+    tile_body<Pol, TX, TY, MODE>(sc.P, sc.K, sc.A, sc.R, t, sc.R.tmap, true, part, true);
     if (MODE == kModeFull && sc.R.cost) {
         __syncthreads();
         if (threadIdx.x == 0) {
