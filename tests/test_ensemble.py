@@ -96,6 +96,36 @@ def test_ensemble_split_tiles_match_cases_run_alone(form):
 
 
 @pytest.mark.gpu
+def test_ensemble_cases_of_different_grids():
+    """Cases on grids of different sizes (and so different tile counts) in
+    one ensemble each end where they end alone."""
+    n, rebin = 11, 4
+    specs = [((96, 48), 0.75, (40, 10), 3), ((64, 32), 0.5, (24, 8), 5), ((128, 40), 1.0, (56, 8), 9)]
+    cases = []
+    for grid, dim, cells, seed in specs:
+        p = params(*grid, dim=dim)
+        cases.append((p, scene(p, cells=cells, seed=seed, ind_y=0.03, vel=0.05, perturb=5e-4)))
+    ens = Ensemble(im.FORM_FP64, tile=1, threads=128)
+    ens.set(rebin_interval=rebin)
+    models = []
+    for p, soa in cases:
+        m = gpu_model(p, soa, im.FORM_FP64, tile=1, threads=128)
+        ens.add(m)
+        models.append(m)
+    ens.run(n)
+    for (p, soa), m in zip(cases, models):
+        got, hist = gpu_state(m), m.gpu.force_history(n)
+        _, ref, href = _alone(p, soa, im.FORM_FP64, n, rebin)
+        err = compare_states(p, got, ref, soa)
+        assert err["disp_h"] <= 1e-9 and err["strain"] <= 1e-9 and err["vel"] <= 1e-9, err
+        assert np.abs(hist - href).max() <= 1e-6 * max(np.abs(href).max(), 1e-30)
+        assert m.gpu.error_code == 0
+    ens.close()
+    for m in models:
+        m.gpu.close()
+
+
+@pytest.mark.gpu
 def test_ensemble_runs_compose():
     """Two ensemble runs continue each other (a second run re-packs nothing
     and reuses its captured graph)."""
