@@ -43,6 +43,14 @@ def test_null_arguments_are_errors_not_crashes():
     assert b"null" in L.icm_last_error()
     assert L.icm_transfer_points_to_device(None, None) == 2
     assert L.icm_scene_block(None, None, None, None) == 2
+    assert L.icm_set_tile_split(None, 64, 1.3) == 2
+    from icempm_b200 import ensemble as ens
+
+    E = ens._sigs()
+    assert E.icm_ensemble_set_split(None, 64, 1.3) == 2
+    assert E.icm_ensemble_set(None, 200, 1) == 2
+    assert E.icm_ensemble_run(None, None, 1) == 2
+    assert E.icm_ensemble_size(None) == -1
 
 
 @pytest.mark.skipif(os.path.exists("/dev/nvidia0"), reason="checks the no-device error path")
