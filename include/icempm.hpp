@@ -200,6 +200,16 @@ public:
     }
     inline void run_substeps(int n);
     void run_substeps(icy_SimParams &p, int n) { icy::icm_check(icm_run_substeps(ctx_, &p, n)); }
+    void set_rebin_interval(int substeps)
+    {
+        initialize();
+        icy::icm_check(icm_set_rebin_interval(ctx_, substeps));
+    }
+    void set_tile_split(int max_tiles, double ratio)
+    {
+        initialize();
+        icy::icm_check(icm_set_tile_split(ctx_, max_tiles, ratio));
+    }
     icm_ctx *context() const { return ctx_; }
 
 private:
@@ -267,6 +277,51 @@ public:
 private:
     bool abortRequested = false;
 };
+
+namespace icy {
+/* Many cases advanced together, one launch per substep for all of them
+ * (icm_ensemble_*); no counterpart in the reference, which runs one case per
+ * process. Each case is a Model set up as for Step (block loaded, constants
+ * updated); run(n) advances every case n substeps and leaves its results
+ * in the case, as GPU_Implementation5::run_substeps would. */
+class Ensemble {
+public:
+    explicit Ensemble(int form = ICM_FORM_FP32, int tile_variant = 1, int threads = 128, int device = 0)
+    {
+        icm_check(icm_ensemble_create(&e_, device, form, tile_variant, threads));
+    }
+    Ensemble(const Ensemble &) = delete;
+    Ensemble &operator=(const Ensemble &) = delete;
+    ~Ensemble()
+    {
+        if (e_) icm_ensemble_destroy(e_);
+    }
+    void add(Model &m)
+    {
+        m.gpu.initialize();
+        icm_check(icm_ensemble_add(e_, m.gpu.context()));
+        cases_.push_back(&m);
+    }
+    void set(int rebin_interval, bool graphs = true) { icm_check(icm_ensemble_set(e_, rebin_interval, graphs ? 1 : 0)); }
+    void set_split(int max_tiles, double ratio) { icm_check(icm_ensemble_set_split(e_, max_tiles, ratio)); }
+    void run(int n)
+    {
+        std::vector<icy_SimParams *> p;
+        for (Model *m : cases_) p.push_back(&m->prms);
+        icm_check(icm_ensemble_run(e_, p.data(), n));
+    }
+    void synchronize()
+    {
+        for (Model *m : cases_) m->gpu.synchronize();
+    }
+    void *stream() const { return icm_ensemble_stream(e_); }
+    size_t size() const { return cases_.size(); }
+
+private:
+    icm_ensemble *e_ = nullptr;
+    std::vector<Model *> cases_;
+};
+}  // namespace icy
 
 /* icy::SnapshotManager (snapshotmanager.h:15-31) over the library's HDF5
  * code. ReadSnapshot resumes a run (the reference's is commented out). */

@@ -91,3 +91,54 @@ def test_shim_frame_matches_python_model(shim_exe, tmp_path, form):
         scale = max(np.abs(b[row]).max(), 1e-30)
         assert np.abs(a[row] - b[row]).max() <= row_tol * scale, row
     assert np.array_equal(got.reshape(16, pitch)[0].view(np.uint8)[:n], want.reshape(16, pitch)[0].view(np.uint8)[:n])
+
+
+@pytest.fixture(scope="module")
+def shim_ens_exe(tmp_path_factory):
+    out = tmp_path_factory.mktemp("shim_ens") / "shim_ensemble"
+    lib_dir = os.path.dirname(build.LIB)
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "shim_ensemble.cpp"), "-L", lib_dir, "-licempm",
+                    f"-Wl,-rpath,{lib_dir}", "-o", str(out)], check=True)
+    return str(out)
+
+
+def test_shim_ensemble_compiles_and_fails_cleanly_without_device(shim_ens_exe, tmp_path):
+    cfg, _ = _config(tmp_path)
+    r = subprocess.run([shim_ens_exe, cfg, str(tmp_path / "o"), "3", *map(str, CELLS)], capture_output=True, text=True)
+    assert r.returncode in (0, 3), r.stdout + r.stderr
+    if r.returncode == 3:
+        assert "no device:" in r.stdout
+
+
+@pytest.mark.gpu
+def test_shim_ensemble_matches_cases_run_alone(shim_ens_exe, tmp_path):
+    """icy::Ensemble over two Models ends each case where the Python model
+    of the same scene ends when run alone (FP32 form)."""
+    cfg_path, cfg = _config(tmp_path)
+    n = 9
+    r = subprocess.run([shim_ens_exe, cfg_path, str(tmp_path / "o"), str(n), *map(str, CELLS)], capture_output=True,
+                       text=True)
+    assert r.returncode == 0 and "ensemble ok" in r.stdout, r.stdout + r.stderr
+    for i in range(2):
+        got = np.fromfile(str(tmp_path / f"o.{i}"), dtype=np.float64)
+        m = im.Model(0)
+        p = im.SimParams()
+        p.Reset()
+        p.ParseString(json.dumps(cfg))
+        m.prms = p
+        m.gpu.model = m
+        m.load_block(CELLS[0] + 8 * i, CELLS[1], ind_y_above_floor=0.05, grain_size=0.02, seed=7 + i)
+        m.gpu.set_form(im.FORM_FP32)
+        m.gpu.set_tile(1, 128)
+        m.gpu.set_rebin_interval(4)
+        m.gpu.run_substeps(m.prms, n)
+        m.gpu.cuda_transfer_from_device()
+        m.gpu.synchronize()
+        want = m.gpu.tmp_transfer_buffer.copy()
+        pitch, npts = int(m.prms.nPtsPitch), int(m.prms.nPts)
+        m.gpu.close()
+        assert got.size == want.size
+        a, b = got.reshape(16, pitch)[:, :npts], want.reshape(16, pitch)[:, :npts]
+        assert np.abs(a[4:6] - b[4:6]).max() <= 1e-5 * m.prms.cellsize
+        assert np.abs(a[8:12] - b[8:12]).max() <= 1e-4 * max(np.abs(b[8:12] - np.array([1, 0, 0, 1.0])[:, None]).max(), 1e-12)
