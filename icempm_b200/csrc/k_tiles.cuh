@@ -117,13 +117,13 @@ constexpr int kTmaPolls = 1 << 22;
 // a multiple of 16 bytes for any rx0, negative ones included. Thread 0
 // issues the copy; every thread of the CTA must later call tma_region_wait
 // (the CTA may not exit with the copy in flight).
-__device__ __forceinline__ void tma_region_issue(const CUtensorMap *map, bool map_in_global, void *dst, int rx0,
-                                                 int ry0, uint32_t bytes, uint64_t *bar)
+// (A descriptor in global memory must have been fenced for the tensor-map
+// proxy by the issuing thread before this; one in kernel parameters needs
+// nothing.)
+__device__ __forceinline__ void tma_region_issue(const CUtensorMap *map, void *dst, int rx0, int ry0, uint32_t bytes,
+                                                 uint64_t *bar)
 {
     if (threadIdx.x == 0) {
-        // a descriptor in global memory (written by a host copy) is fenced
-        // for the tensor-map proxy; one in kernel parameters needs nothing
-        if (map_in_global) asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
         tc05::mbar_init(bar, 1);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc05::smem_u32(bar)), "r"(bytes)
                      : "memory");
@@ -751,6 +751,17 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         __syncwarp();
         if (MODE != kModeP2GOnly) Pol::init_tables(s_tab, K, tid, nthr);
     }
+    // a full substep of a tile with particles stages its node region with
+    // one tensor copy (below, after the wait); a descriptor in global memory
+    // (written by a host copy before the launch) is fenced for the
+    // tensor-map proxy here, so that the fence overlaps the wait
+    bool staging = false;
+    if constexpr (MODE == kModeFull) {
+        staging = p1 > p0 && tmaps && tile_region_bytes<Pol, MODE>(RN, nthr >> 5) >= RN * sizeof(Node) &&
+                  (tc05::smem_u32(s_dyn) & 127u) == 0;
+        if (staging && tmaps_in_global && tid == 0)
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmaps + R.bufA) : "memory");
+    }
     // launched as a programmatic dependent: wait until the previous kernel
     // of the stream has completed and its writes are visible, then let the
     // next one launch (its CTAs take free slots, set up, and wait here)
@@ -758,16 +769,11 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         asm volatile("griddepcontrol.wait;" ::: "memory");
         asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     }
-    // a full substep of a tile with particles stages its node region with
-    // one tensor copy into the (not yet used) accumulation regions, issued
-    // here so that it lands while the tile zeroes and sets up
-    bool staging = false;
+    // the node region's copy into the (not yet used) accumulation regions,
+    // issued right after the wait so that it lands while the tile zeroes
+    // its next-but-one buffer
     if constexpr (MODE == kModeFull) {
-        staging = p1 > p0 && tmaps && tile_region_bytes<Pol, MODE>(RN, nthr >> 5) >= RN * sizeof(Node) &&
-                  (tc05::smem_u32(s_dyn) & 127u) == 0;
-        if (staging)
-            tma_region_issue(tmaps + R.bufA, tmaps_in_global, s_dyn, rx0, ry0, (uint32_t)(RN * sizeof(Node)),
-                             &s_tma_bar);
+        if (staging) tma_region_issue(tmaps + R.bufA, s_dyn, rx0, ry0, (uint32_t)(RN * sizeof(Node)), &s_tma_bar);
     }
 
     // 1. zero this tile in the buffer the next substep will scatter into;
