@@ -8,6 +8,7 @@ import socket
 import subprocess
 import sys
 
+import pytest
 import torch.multiprocessing as mp
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -79,3 +80,28 @@ def test_reference_arm_rank0_prints_one_line():
     assert d["impl"] == "reference" and d["unit"] == "particle-updates/s" and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+@pytest.mark.gpu
+def test_bench_line_carries_the_contract_keys():
+    """One short bench run on the GPU prints one JSON line with every key the
+    measurement contract names (the sections that take minutes are off)."""
+    r = _run_bench({"RANK": "0", "WORLD_SIZE": "1", "LOCAL_RANK": "0"}, "--steps", "1", "--warmup", "3",
+                   "--substeps", "10", "--config", "c1_70k", "--tile", "1", "--no-accuracy", "--no-fp64",
+                   "--no-ensemble", "--no-cpu")
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "gpu_launches", "roofline", "clocks", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["value"] > 0 and d["n_gpus"] == 1 and d["gpu_launches"] == 1 * (10 + 2)
+    for k in ("bound", "achieved", "peak", "unit", "frac", "traffic"):
+        assert k in d["roofline"], k
+    for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step"):
+        assert k in d["e2e"], k
+    assert d["e2e"]["h2d_bytes_per_step"] > 0 and d["e2e"]["d2h_bytes_per_step"] > 0
+    for k in ("sm_mhz", "sm_max_mhz", "reasons"):
+        assert k in d["clocks"], k
+    assert "workload" in d["config"]
