@@ -51,7 +51,9 @@ class Ensemble:
         _check(_sigs().icm_ensemble_set(self._e, rebin_interval, 1 if graphs else 0))
 
     def set_split(self, max_tiles: int = 128, ratio: float = 1.3) -> None:
-        """Heavy tiles run as two CTAs (max_tiles 0, the default: off)."""
+        """Heavy tiles run as two CTAs. An ensemble starts with this off;
+        set_split() turns it on with the single-run defaults, max_tiles 0
+        turns it off again."""
         _check(_sigs().icm_ensemble_set_split(self._e, max_tiles, ratio))
 
     def run(self, n: int) -> None:
