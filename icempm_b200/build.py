@@ -78,14 +78,17 @@ def build_cli(force: bool = False) -> str:
 
 
 def build_oracle(force: bool = False) -> None:
-    """Builds the CPU oracle and, when the reference checkout is present, its
-    SVD harness (test infrastructure)."""
+    """Builds the CPU oracle and, when the reference checkout is present, the
+    reference's own SVD and substep code for the host (oracle/_ref; test
+    infrastructure)."""
     target = os.path.join(ORACLE, "libmpm_oracle.so")
     if force or _stale(target, [os.path.join(ORACLE, "mpm_oracle.c"),
                                 os.path.join(ROOT, "include", "icempm_params.h")]):
         _run(["make", "-C", ORACLE, "libmpm_oracle.so"] + (["-B"] if force else []))
-    ref = os.path.join(ORACLE, "_ref", "libref_svd.so")
-    if force or not os.path.exists(ref):
+    refs = [os.path.join(ORACLE, "_ref", f) for f in ("libref_svd.so", "libref_step.so")]
+    srcs = [os.path.join(ORACLE, f) for f in ("build_ref.sh", "ref_svd_harness.cpp", "ref_step_harness.cpp",
+                                               "ref_step_pre.h", os.path.join("ref_stub", "Eigen", "Core"))]
+    if force or any(_stale(r, srcs) for r in refs):
         _run(["sh", os.path.join(ORACLE, "build_ref.sh")])
 
 

@@ -132,6 +132,10 @@ struct icm_ctx {
     long long ktime_count = 0;
 
     bool ref_valid = true, internal_valid = false, internal_pq = false;
+    // the next fused launch may be a programmatic dependent of the kernel
+    // before it: false after a kernel whose writes (launch order, re-binned
+    // cells and groups) the substep reads before its griddepcontrol.wait
+    bool pdl_next = false;
     int internal_variant = -1;
     int nslots = 0;
     int *h_ns = nullptr;  // pinned: the slot count a re-binning reads back
@@ -489,8 +493,9 @@ static int launch_one(icm_ctx *c, int ntiles, const icy_SimParams &P, const type
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = c->pdl_next ? 1 : 0;
     ICM_CUDA(cudaLaunchKernelEx(&cfg, k_tile_substep<Pol, TX, TY, MODE>, P, K, A, R, c->h_tmap));
+    c->pdl_next = true;
     ICM_LAUNCHED("k_tile_substep");
     return ICM_OK;
 }
@@ -650,6 +655,7 @@ static int rebin_internal(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
     int rc = rebin_begin(c, P);
     if (rc) return rc;
     ICM_CUDA(cudaStreamSynchronize(c->stream));
+    c->pdl_next = false;  // the substep reads cells and groups before its dependency wait
     return rebin_finish(c, P, keep_pq);
 }
 
@@ -741,6 +747,7 @@ static int tile_order(icm_ctx *c, int ntiles, const int *&order, int &nlaunch)
     k_tile_order<<<1, kOrderThreads, sizeof(unsigned long long) * m, c->stream>>>(
         ntiles, c->fz.cost, c->bin.tile_start, max_split, (float)c->split_ratio, c->fz.order);
     ICM_LAUNCHED("k_tile_order");
+    c->pdl_next = false;  // the substep reads the order before its dependency wait
     order = c->fz.order;
     nlaunch = ntiles + max_split;
     return ICM_OK;
@@ -764,6 +771,7 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     const size_t nnodes = (size_t)P.GridX * P.GridY;
     const size_t node_bytes = (storage_form(c->form) == ICM_FORM_FP64) ? sizeof(Node64) : sizeof(float4);
     cudaStream_t s = c->stream;
+    c->pdl_next = false;  // packing or an earlier run's kernels precede the prologue
     for (int b = 0; b < 3; b++) ICM_CUDA(cudaMemsetAsync(c->fz.grid[b], 0, node_bytes * nnodes, s));
     ICM_CUDA(cudaMemsetAsync(c->fz.dirty, 0, 3 * (size_t)ntiles, s));
     int rc = ensure_hist(c, n);
@@ -1315,6 +1323,10 @@ constexpr int kEnsGraphs = 4;
 template <class Pol, int TX, int TY, int MODE>
 int ens_launch_one(icm_ensemble *e, int grid, const void *d_cases, const EnsLaunch &L)
 {
+    // the first launch of a segment, the prologue and the final launch follow
+    // k_set_int or the descriptor upload, whose writes the kernel reads before
+    // its dependency wait: they are ordinary stream-ordered launches
+    const bool pdl = MODE == kModeFull && L.j > 0;
     constexpr int RN = (TX + 4) * (TY + 4);
     const int nwarps = e->threads / 32;
     const size_t dyn = tile_dyn_bytes<Pol, MODE>(RN, nwarps);
@@ -1336,7 +1348,7 @@ int ens_launch_one(icm_ensemble *e, int grid, const void *d_cases, const EnsLaun
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = pdl ? 1 : 0;
     ICM_CUDA(cudaLaunchKernelEx(&cfg, k_tile_substep_ens<Pol, TX, TY, MODE>, static_cast<const EnsCase<Pol> *>(d_cases),
                                 L));
     ICM_LAUNCHED("k_tile_substep_ens");
@@ -1523,9 +1535,12 @@ int ens_active_tiles(icm_ensemble *e, const std::vector<icy_SimParams> &P)
         }
         for (int t = 0; t < ntiles; t++)
             if (busy[t]) {
-                const unsigned long long cc = (unsigned long long)cost[t] + cost[(size_t)ntiles + t];
+                // a tile without particles (its cost may be one measured
+                // before a re-binning emptied it) sorts last and is never split
+                const bool has_pts = ts[t + 1] > ts[t];
+                const unsigned long long cc = has_pts ? (unsigned long long)cost[t] + cost[(size_t)ntiles + t] : 0ull;
                 items.push_back({cc > 0xffffffffull ? 0xffffffffu : (unsigned)cc, (int)i, t});
-                if (ts[t + 1] > ts[t]) {
+                if (has_pts) {
                     busy_sum += cc;
                     nbusy++;
                 }

@@ -850,8 +850,9 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                     s_v[k].y = v1;
                 }
             }
-        } else if (contact_possible) {
+        } else if (contact_possible && part != 2) {
             // no particles here: only the reaction of this tile's own nodes
+            // (counted once, by the first half when the tile runs split)
             for (int k = tid; k < TX * TY; k += nthr) {
                 const int gx = x0 + k % TX, gy = y0 + k / TX;
                 if (gx < GX && gy < GY) {
@@ -1347,13 +1348,13 @@ __global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsig
     int busy = 0;
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
         unsigned c = 0;
-        if (i < n) {
+        // a tile without particles (its cost may still be the one measured
+        // before a re-binning emptied it) sorts last and is never split
+        if (i < n && tile_start[i + 1] > tile_start[i]) {
             const unsigned long long cc = (unsigned long long)cost[i] + cost[n + i];
             c = cc > 0xffffffffull ? 0xffffffffu : (unsigned)cc;
-            if (tile_start[i + 1] > tile_start[i]) {
-                sum += c;
-                busy++;
-            }
+            sum += c;
+            busy++;
         }
         s_key[i] = (i < n) ? (((unsigned long long)c << 32) | (0xffffffffu - (unsigned)i)) : 0ull;
     }

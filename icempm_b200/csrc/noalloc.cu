@@ -40,23 +40,34 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_noalloc_grid[3 * kNoAllocMaxNodes];
 
 // Device address of g_noalloc_grid per device. In host code the symbol is
-// only a host-side stand-in; the kernels must be given this address.
+// only a host-side stand-in; the kernels must be given this address. It is
+// looked up again (cudaGetSymbolAddress, with the device current) on every
+// call made outside stream capture, so that a context created anew on the
+// device (after cudaDeviceReset, say) gets its own address; a call made
+// while its stream is being captured takes the address of the last call on
+// the device, which must have come before the capture began.
 std::mutex g_setup_mutex;
 double *g_grid_addr[kMaxDevices] = {};
 
-int grid_address(double **out)
+int grid_address(cudaStream_t s, double **out)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return icm::fail(ICM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return icm::fail(ICM_ERR_ARG, "icm_run_substeps_noalloc: device index too large");
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cs);
+    if (e != cudaSuccess) return icm::fail(ICM_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_grid_addr[dev]) {
+    if (cs == cudaStreamCaptureStatusNone) {
         void *ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_noalloc_grid);
         if (e != cudaSuccess || !ptr)
             return icm::fail(ICM_ERR_CUDA, std::string("cudaGetSymbolAddress(grid scratch): ") + cudaGetErrorString(e));
         g_grid_addr[dev] = static_cast<double *>(ptr);
+    } else if (!g_grid_addr[dev]) {
+        return icm::fail(ICM_ERR_STATE,
+                         "icm_run_substeps_noalloc: the first call on a device must come before any stream capture");
     }
     *out = g_grid_addr[dev];
     return ICM_OK;
@@ -79,12 +90,12 @@ extern "C" int icm_run_substeps_noalloc(icy_SimParams *p, double *pts, double *b
     if (p->n_indenter_subdivisions < 1) return icm::fail(ICM_ERR_ARG, "icm_run_substeps_noalloc: no force bins");
     if (!(p->cellsize > 0) || !(p->InitialTimeStep > 0) || p->UpdateEveryNthStep < 1)
         return icm::fail(ICM_ERR_ARG, "icm_run_substeps_noalloc: cellsize, time step or frame length not positive");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     double *grid = nullptr;
-    int rc = grid_address(&grid);
+    int rc = grid_address(s, &grid);
     if (rc) return rc;
     if (n == 0) return ICM_OK;
 
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     icy_SimParams P = *p;
     P.grid_array = grid;
     P.nGridPitch = nodes;

@@ -205,9 +205,11 @@ void *icm_stream(icm_ctx *ctx);
  * GridX*GridY may be at most 262,144 nodes (6 MiB, held by every GPU that
  * loads the library until exit); larger grids are rejected with
  * ICM_ERR_ARG. All calls share that scratch, so calls that overlap on the
- * GPU race and must not be issued concurrently. The first call on a device
- * looks up the scratch's device address; make that first call before any
- * stream capture. */
+ * GPU race and must not be issued concurrently. Each call made outside
+ * stream capture looks up the scratch's device address in the current
+ * context (so a context re-created after cudaDeviceReset gets its own); a
+ * call on a stream under capture reuses the address of the device's last
+ * call, so make the first call on a device before any stream capture. */
 int icm_run_substeps_noalloc(icy_SimParams *p, double *pts, double *bins, int *err, int n, void *stream);
 /* ------------------------------------------------ learned projection
  * No counterpart in the reference. A 6 -> 64 -> 64 -> 3 GELU network

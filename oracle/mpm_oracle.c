@@ -32,10 +32,13 @@
  * Here such contributions are dropped and the error indicator is raised; G2P
  * reads an out-of-grid node as zero velocity.
  *
- * Parity pin: the 2x2 SVD is checked against the reference's own
- * helper_math.cuh/givens.cuh compiled for the host (oracle/build_ref.sh).
- * The rest of the device math has no golden vectors in the reference (it has
- * no tests); it is pinned only by this restatement.
+ * Parity pin: every function above and the whole substep are checked
+ * against the reference's own code compiled for the host
+ * (oracle/build_ref.sh: helper_math.cuh/givens.cuh into libref_svd.so;
+ * gpu_implementation5.cu:1-416 with an Eigen-subset stub into
+ * libref_step.so). With one thread the results agree bit for bit on scenes
+ * whose stencils stay inside the grid; the force bins, which this file sums
+ * per substep before adding them, agree to rounding.
  *
  * Parallelism: OpenMP. P2G scatters into per-thread private node bands that
  * are summed in thread order, so results are deterministic for a fixed
@@ -282,6 +285,39 @@ static void drucker_prager(const icy_SimParams *P, const pq_t *o, double Fe[4], 
             usvt(o->U, s_new, o->V, Fe);
         }
     }
+}
+
+/* Exports of the single functions for the per-function pin against the
+ * reference's own code (tests/test_oracle.py). out: U[4], sigma[2], V[4],
+ * Je_tr, p_tr, q_tr, sigma^2[2], s_hat[2] (17 doubles). */
+void oracle_compute_pq(const icy_SimParams *P, const double Fe[4], double out[17])
+{
+    pq_t o;
+    compute_pq(P, Fe, &o);
+    for (int i = 0; i < 4; i++) {
+        out[i] = o.U[i];
+        out[6 + i] = o.V[i];
+    }
+    out[4] = o.S[0];
+    out[5] = o.S[1];
+    out[10] = o.Je_tr;
+    out[11] = o.p_tr;
+    out[12] = o.q_tr;
+    out[13] = o.S2[0];
+    out[14] = o.S2[1];
+    out[15] = o.s_hat[0];
+    out[16] = o.s_hat[1];
+}
+
+/* out: pmin, pmax, qmax, beta, mSq */
+void oracle_grain_params(const icy_SimParams *P, short grain, double out[5])
+{
+    grain_params(P, grain, &out[0], &out[1], &out[2], &out[3], &out[4]);
+}
+
+int oracle_failure_check(const icy_SimParams *P, short grain, double p, double q)
+{
+    return failure_check(P, grain, p, q);
 }
 
 /* The part of v2_kernel_g2p after the Fe update (gpu_implementation5.cu:353-356):

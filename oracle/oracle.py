@@ -14,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmpm_oracle.so")
 REF_SVD_PATH = os.path.join(HERE, "_ref", "libref_svd.so")
+REF_STEP_PATH = os.path.join(HERE, "_ref", "libref_step.so")
 
 _L = None
 
@@ -37,6 +38,9 @@ def lib():
             "oracle_g2p": (None, [P, vp, vp, i, i]),
             "oracle_run_substeps": (i, [P, vp, vp, vp, vp, i, i]),
             "oracle_max_threads": (i, []),
+            "oracle_compute_pq": (None, [P, vp, vp]),
+            "oracle_grain_params": (None, [P, C.c_short, vp]),
+            "oracle_failure_check": (i, [P, C.c_short, d, d]),
         }
         for n, (r, a) in sigs.items():
             f = getattr(L, n)
@@ -54,6 +58,53 @@ def ref_svd_lib():
     L.ref_svd.restype = None
     L.ref_svd.argtypes = [C.c_void_p] * 4
     return L
+
+
+_RS = None
+
+
+def ref_step_lib():
+    """The reference's own device functions and kernel bodies
+    (gpu_implementation5.cu:1-416) compiled for the host by
+    oracle/build_ref.sh, or None if not built."""
+    global _RS
+    if _RS is None and os.path.exists(REF_STEP_PATH):
+        L = C.CDLL(REF_STEP_PATH)
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        sigs = {
+            "ref_params_size": (i, []),
+            "ref_kirchhoff": (None, [vp, vp, vp]),
+            "ref_compute_pq": (None, [vp, vp, vp]),
+            "ref_grain_params": (None, [vp, C.c_short, vp]),
+            "ref_failure_check": (i, [vp, C.c_short, d, d]),
+            "ref_constitutive": (None, [vp, vp, vp, vp, C.c_short, vp, vp]),
+            "ref_run_substeps": (i, [vp, vp, vp, vp, i]),
+        }
+        for n, (r, a) in sigs.items():
+            f = getattr(L, n)
+            f.restype = r
+            f.argtypes = a
+        _RS = L
+    return _RS
+
+
+def compute_pq(prms, F):
+    """ComputePQ: U[4], sigma[2], V[4], Je_tr, p_tr, q_tr, sigma^2[2],
+    s_hat[2] as one array of 17."""
+    F = np.ascontiguousarray(F, dtype=np.float64).reshape(4)
+    out = np.zeros(17)
+    lib().oracle_compute_pq(C.byref(prms), _p(F), _p(out))
+    return out
+
+
+def grain_params(prms, grain):
+    out = np.zeros(5)
+    lib().oracle_grain_params(C.byref(prms), int(grain), _p(out))
+    return out
+
+
+def failure_check(prms, grain, p, q) -> int:
+    return int(lib().oracle_failure_check(C.byref(prms), int(grain), float(p), float(q)))
 
 
 def _p(a: np.ndarray):

@@ -8,6 +8,20 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 
+def reference_root():
+    """The reference checkout for tests that read its data files: the
+    ICEMPM_REFERENCE environment variable, else the location that
+    oracle/build_ref.sh recorded when it built oracle/_ref; None when
+    neither names an existing directory (the tests then skip)."""
+    root = os.environ.get("ICEMPM_REFERENCE")
+    if not root:
+        rec = os.path.join(ROOT, "oracle", "_ref", "reference_root")
+        if os.path.exists(rec):
+            with open(rec) as f:
+                root = f.read().strip()
+    return root if root and os.path.isdir(root) else None
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 

@@ -1,0 +1,73 @@
+"""GPU forms against the CPU FP64 oracle on the configurations the
+reference's step is quoted on, over long horizons.
+
+* 69,632 particles on the 512x128 grid (dt 2e-6): 10,000 substeps, the
+  length of the workload, with checkpoints after 1, 10, 100, 1,000 and
+  10,000 substeps;
+* 999,424 particles on the 2048x512 grid (dt 5e-7): 200 substeps, with
+  checkpoints after 1, 10, 100 and 200.
+
+The FP64 forms must track the oracle to rounding (float atomics reorder the
+P2G and force sums, so bit-exactness is out of reach): positions within
+1e-8 h, velocity, Fe and the per-substep force history within 1e-7 of their
+scales, Jp_inv within 1e-9, identical crushed flags. The FP32 form is held
+to the north-star bars where they apply at these horizons: positions within
+1e-3 h and peak force within 1 %. Each test prints its errors as one JSON
+line (prefix PARITY).
+"""
+import json
+import os
+
+import pytest
+
+import icempm_b200 as im
+from icempm_b200 import configs
+from tests.tracking import track
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = {"x_max_h": 1e-8, "v_rel": 1e-7, "Fe_rel": 1e-7, "Jp_inv_abs": 1e-9}
+FP64_FORCE_TOL = 1e-7
+
+
+def _threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def _check_fp64(res, name, checkpoints):
+    for c in checkpoints:
+        e = res[name][str(c)]
+        for k, tol in FP64_TOL.items():
+            assert e[k] <= tol, (name, c, k, e)
+        assert e["crushed_mismatch"] == 0, (name, c, e)
+    assert res[name]["force"]["history_max_rel"] <= FP64_FORCE_TOL, (name, res[name]["force"])
+    assert res[name]["error_word"] == 0
+
+
+def test_70k_fp64_forms_track_the_oracle_over_10k_substeps():
+    p, soa = configs.make_scene("c1_70k")
+    cps = (1, 10, 100, 1000, 10000)
+    res = track(p, soa, (im.FORM_FP64_STEPWISE, im.FORM_FP64, im.FORM_FP32), cps, _threads())
+    print("PARITY", json.dumps({"workload": "c1_70k", "substeps": cps[-1], "errors": res}))
+    assert res["oracle_error_word"] == 0
+    _check_fp64(res, "fp64-stepwise", cps)
+    _check_fp64(res, "fp64", cps)
+    f32 = res["fp32"]
+    assert f32["10000"]["x_max_h"] <= 1e-3 and f32["force"]["peak_rel"] <= 1e-2, f32
+    assert f32["error_word"] == 0
+
+
+def test_1m_forms_track_the_oracle_over_200_substeps():
+    p, soa = configs.make_scene("c3_1m")
+    cps = (1, 10, 100, 200)
+    res = track(p, soa, (im.FORM_FP64_STEPWISE, im.FORM_FP64, im.FORM_FP32), cps, _threads())
+    print("PARITY", json.dumps({"workload": "c3_1m", "substeps": cps[-1], "errors": res}))
+    assert res["oracle_error_word"] == 0
+    _check_fp64(res, "fp64-stepwise", cps)
+    _check_fp64(res, "fp64", cps)
+    f32 = res["fp32"]
+    assert f32["200"]["x_max_h"] <= 1e-3 and f32["force"]["peak_rel"] <= 1e-2, f32
+    assert f32["error_word"] == 0

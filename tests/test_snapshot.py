@@ -15,7 +15,10 @@ from oracle import oracle as orc
 from h5_check import H5
 from mpm_cases import gpu_model, gpu_state, params, scene
 
-FIXTURES = [os.path.join(os.sep, "root", "reference", "geometries_2d", f) for f in ("2d_70k.h5", "2d_250k.h5")]
+from conftest import reference_root
+
+_REF = reference_root()
+FIXTURES = [os.path.join(_REF, "geometries_2d", f) for f in ("2d_70k.h5", "2d_250k.h5")] if _REF else []
 ATTRS = ["indenter_x", "indenter_y", "SimulationTime", "GridX", "GridY", "nPts", "nPtsPitch", "UpdateEveryNthStep",
          "n_indenter_subdivisions", "cellsize", "IndDiameter", "InitialTimeStep", "SetupType", "Volume"]
 
@@ -126,7 +129,7 @@ def test_repitch_soa_moves_grains_and_crushed():
     assert np.array_equal(A.rows[1:, :n], B.rows[1:, :n])
 
 
-@pytest.mark.skipif(not os.path.exists(FIXTURES[0]), reason="reference fixtures not present")
+@pytest.mark.skipif(not FIXTURES or not os.path.exists(FIXTURES[0]), reason="reference fixtures not present")
 @pytest.mark.parametrize("path", FIXTURES)
 def test_raw_points_loader_matches_independent_parser(path):
     """LoadRawPoints on a file written by the HDF5 library (chunked,

@@ -4,8 +4,9 @@ It serves callers that cannot allocate device memory while they run (an
 allocation can block or synchronise the device, or another allocator owns
 the GPU's memory). Its grid scratch is a fixed array inside the library, so
 this test checks, through the C ABI, that two calls in a row give what the
-allocating entry point gives on the same input, within the FP64 tolerance
-of the other parity tests (1e-9), and that an oversized grid is refused.
+allocating entry point gives on the same input, and what the CPU oracle
+gives on the 69,632-particle 512x128 workload, within the FP64 tolerance of
+the other parity tests (1e-9), and that an oversized grid is refused.
 """
 import ctypes as C
 
@@ -64,6 +65,35 @@ def test_noalloc_matches_allocating_entry_point_twice():
     assert int(err.item()) == 0
     assert q.SimulationStep == ref_params.SimulationStep == 2 * n
     assert q.SimulationTime == ref_params.SimulationTime and q.indenter_x == ref_params.indenter_x
+
+
+def test_noalloc_matches_the_oracle_on_the_70k_workload():
+    """69,632 particles on the 512x128 grid (65,536 nodes, inside the
+    scratch), 20 substeps in two calls, against the CPU oracle at the FP64
+    tolerance of the other parity tests (the GPU's atomics reorder sums)."""
+    import torch
+
+    from icempm_b200 import configs
+    from tests.mpm_cases import oracle_run
+
+    p, soa = configs.make_scene("c1_70k")
+    n = 10
+    q_ref, ref, ref_bins, err_ref, _ = oracle_run(p, soa, 2 * n, threads=8)
+    f = _noalloc()
+    q = p.copy()
+    pts = torch.tensor(soa, dtype=torch.float64, device="cuda")
+    bins = torch.zeros(2 * q.n_indenter_subdivisions, dtype=torch.float64, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for _ in range(2):
+        rc = f(C.byref(q), pts.data_ptr(), bins.data_ptr(), err.data_ptr(), n, None)
+        assert rc == 0, im.library().icm_last_error()
+    torch.cuda.synchronize()
+    e = compare_states(p, pts.cpu().numpy(), ref, soa)
+    assert e["crushed_mismatch"] == 0 and e["grain_mismatch"] == 0
+    assert max(e["disp_rel"], e["vel"], e["strain"], e["Bp"], e["Jp"]) < TOL, e
+    assert np.abs(ref_bins).max() > 0 and max_rel(bins.cpu().numpy(), ref_bins) < TOL
+    assert int(err.item()) == err_ref == 0
+    assert q.SimulationStep == q_ref.SimulationStep and q.indenter_x == q_ref.indenter_x
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
