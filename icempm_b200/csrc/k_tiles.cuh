@@ -60,18 +60,111 @@ constexpr int kMaxWarps = 8, kMaxGroupsPerWarp = 4;
 
 struct alignas(16) Node64 { double m, px, py, pad; };
 
-// Shared-memory P2G accumulator of one node (one private copy per warp).
+// Shared-memory P2G accumulator of one node (one private copy per warp):
+// {m, px, py} in FP64; {px, py, m, -} in FP32, momentum first so that it
+// sits in an aligned register pair for packed (f32x2) additions.
 struct Acc64 { double m, px, py; };
 __device__ __forceinline__ void acc_zero(float4 &a) { a = make_float4(0.f, 0.f, 0.f, 0.f); }
 __device__ __forceinline__ void acc_zero(Acc64 &a) { a = Acc64{0, 0, 0}; }
-__device__ __forceinline__ void acc_add(float4 &a, float m, float x, float y) { a.x += m; a.y += x; a.z += y; }
+__device__ __forceinline__ void acc_add(float4 &a, float m, float x, float y) { a.x += x; a.y += y; a.z += m; }
 __device__ __forceinline__ void acc_add(Acc64 &a, double m, double x, double y) { a.m += m; a.px += x; a.py += y; }
-__device__ __forceinline__ float acc_m(const float4 &a) { return a.x; }
-__device__ __forceinline__ float acc_x(const float4 &a) { return a.y; }
-__device__ __forceinline__ float acc_y(const float4 &a) { return a.z; }
+__device__ __forceinline__ float acc_m(const float4 &a) { return a.z; }
+__device__ __forceinline__ float acc_x(const float4 &a) { return a.x; }
+__device__ __forceinline__ float acc_y(const float4 &a) { return a.y; }
 __device__ __forceinline__ double acc_m(const Acc64 &a) { return a.m; }
 __device__ __forceinline__ double acc_x(const Acc64 &a) { return a.px; }
 __device__ __forceinline__ double acc_y(const Acc64 &a) { return a.py; }
+// word offsets of m, px, py inside an accumulator
+__device__ __forceinline__ constexpr int acc_off_m(const float4 *) { return 2; }
+__device__ __forceinline__ constexpr int acc_off_x(const float4 *) { return 0; }
+__device__ __forceinline__ constexpr int acc_off_y(const float4 *) { return 1; }
+__device__ __forceinline__ constexpr int acc_off_m(const Acc64 *) { return 0; }
+__device__ __forceinline__ constexpr int acc_off_x(const Acc64 *) { return 1; }
+__device__ __forceinline__ constexpr int acc_off_y(const Acc64 *) { return 2; }
+
+__device__ __forceinline__ float2 bcast2(float a) { return make_float2(a, a); }
+
+// The 27 P2G sums of one cell (mass and momentum of its 3x3 stencil nodes),
+// kept in registers by the lane that owns the cell. add() takes one
+// particle: node (i, j) gets W_ij (m, c + S_h (i, j)^T) with
+// W_ij = wx_i wy_j; flush() adds node (i, j)'s sums to an accumulator.
+template <class real> struct CellSums {
+    real m[9], x[9], y[9];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int q = 0; q < 9; q++) { m[q] = 0; x[q] = 0; y[q] = 0; }
+    }
+    __device__ __forceinline__ void add(const real wx[3], const real wy[3], real mass, real c0, real c1, real S00,
+                                        real S01, real S10, real S11)
+    {
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
+            const real wm = wx[i] * mass;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const real W = wx[i] * wy[j];
+                m[i * 3 + j] += wm * wy[j];
+                x[i * 3 + j] += W * (u0 + S01 * (real)j);
+                y[i * 3 + j] += W * (u1 + S11 * (real)j);
+            }
+        }
+    }
+    template <class Acc> __device__ __forceinline__ void flush(Acc &ac, int i, int j) const
+    {
+        Acc v = ac;
+        acc_add(v, m[i * 3 + j], x[i * 3 + j], y[i * 3 + j]);
+        ac = v;
+    }
+};
+
+// FP32: the momentum sums of a node as one (x, y) pair and the masses of
+// nodes (0, j) and (1, j) as one pair, updated with packed f32x2
+// multiply-adds (two lanes of arithmetic per instruction).
+template <> struct CellSums<float> {
+    float2 xy[9];
+    float2 m01[3];
+    float m2[3];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int q = 0; q < 9; q++) xy[q] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < 3; j++) { m01[j] = make_float2(0.f, 0.f); m2[j] = 0.f; }
+    }
+    __device__ __forceinline__ void add(const float wx[3], const float wy[3], float mass, float c0, float c1, float S00,
+                                        float S01, float S10, float S11)
+    {
+        const float2 c = make_float2(c0, c1), s0 = make_float2(S00, S10), s1 = make_float2(S01, S11);
+        const float2 wx01 = make_float2(wx[0], wx[1]);
+        float2 wyy[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            wyy[j] = bcast2(wy[j]);
+            const float2 mw = __fmul2_rn(bcast2(mass), wyy[j]);
+            m01[j] = __ffma2_rn(mw, wx01, m01[j]);
+            m2[j] = fmaf(mw.x, wx[2], m2[j]);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const float2 u = i == 0 ? c : __ffma2_rn(bcast2((float)i), s0, c);
+            const float2 wxx = bcast2(wx[i]);
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const float2 uj = j == 0 ? u : __ffma2_rn(bcast2((float)j), s1, u);
+                xy[i * 3 + j] = __ffma2_rn(__fmul2_rn(wxx, wyy[j]), uj, xy[i * 3 + j]);
+            }
+        }
+    }
+    __device__ __forceinline__ void flush(float4 &ac, int i, int j) const
+    {
+        float4 v = ac;
+        const float2 s = __fadd2_rn(make_float2(v.x, v.y), xy[i * 3 + j]);
+        const float mm = i == 2 ? m2[j] : (i == 0 ? m01[j].x : m01[j].y);
+        ac = make_float4(s.x, s.y, v.z + mm, v.w);
+    }
+};
 
 struct TileRun {
     int ntx, nty;
@@ -165,7 +258,8 @@ template <class T> struct Tau { T t00, t01, t10, t11; };
 struct Pol64 {
     static constexpr bool kSurrogate = false;
     static constexpr bool kHarvest = false;  // Consts has no harvest fields
-    static constexpr int kMinBlocks = 0;
+    // registers per thread: three 128-thread CTAs per SM
+    static constexpr int kMaxRegs = 168;
     // Bp from raw node velocities, operation order of the reference
     static constexpr bool kRelativeGradient = false;
     using real = double;
@@ -274,7 +368,8 @@ struct Pol64 {
 struct Pol32 {
     static constexpr bool kSurrogate = false;
     static constexpr bool kHarvest = true;
-    static constexpr int kMinBlocks = 0;  // no residency hint: the compiler's own register choice
+    // registers per thread: four 128-thread CTAs per SM
+    static constexpr int kMaxRegs = 128;
     // Bp = 4/h sum W (v_i - v_c) dpos^T with v_c the stencil's centre node:
     // equal to the reference's sum since sum W dpos = 0, but free of the
     // cancellation of a large common velocity (whose FP32 residual would
@@ -428,6 +523,16 @@ struct Pol32 {
         s.H.a10 = H.a10 + (c10 + (c10 * H.a00 + c11 * H.a10));
         s.H.a11 = H.a11 + (c11 + (c10 * H.a01 + c11 * H.a11));
     }
+    // the FP64 redo of a particle that constitutive32 declines
+    static __device__ __forceinline__ void via64(const icy_SimParams &P, St &s, float &p_tr, float &q_tr)
+    {
+        const Via64 o = constitutive32_via64(P, s.H, s.Jp, s.meta);
+        s.H = o.H;
+        s.Jp = o.Jp;
+        s.meta = o.meta;
+        p_tr = o.p_tr;
+        q_tr = o.q_tr;
+    }
     // the trial state of a crushed particle, for the surrogate's training set
     static __device__ __forceinline__ void harvest(const Consts &k, const St &s)
     {
@@ -451,7 +556,7 @@ struct Pol32 {
         Tau32 t;
         if (constitutive32(k, T, s.H, s.meta, p_tr, q_tr, t) == kC32_NEEDS_FP64) {
             harvest(k, s);
-            constitutive32_via64(P, s.H, s.Jp, s.meta, p_tr, q_tr);
+            via64(P, s, p_tr, q_tr);
             redo = 1;
             return stress(P, k, s);
         }
@@ -538,7 +643,6 @@ static __device__ __noinline__ SurrogateOut surrogate_finish(const icy_SimParams
 // Jp_inv < 1, a closed form with nothing to learn), the exact map runs.
 struct Pol32S : Pol32 {
     static constexpr bool kSurrogate = true;
-    static constexpr int kMinBlocks = 0;
     // at most kWarps warps per CTA (128 threads) in this form
     static constexpr int kWarps = 4;
     // A particle held back for the network: slot, state after advection,
@@ -593,7 +697,7 @@ struct Pol32S : Pol32 {
             redo = 2;
             return {0.f, 0.f, 0.f, 0.f};
         }
-        constitutive32_via64(P, s.H, s.Jp, s.meta, p_tr, q_tr);
+        via64(P, s, p_tr, q_tr);
         redo = 1;
         return stress(P, k, s);
     }
@@ -671,6 +775,104 @@ __device__ __noinline__ int far_scatter(const int GX, const int GY, typename Pol
         if (gx < 0 || gy < 0 || gx >= GX || gy >= GY) { bad = 1; continue; }
         node_add_global(g, (size_t)gy * GX + gx, cm[j], cx[j], cy[j]);
         dirty[(gy / TY) * ntx + gx / TX] = 1;
+    }
+    return bad;
+}
+
+// G2P of a particle whose stencil leaves the CTA's node region: velocities
+// recomputed from the scatter buffer node by node. Returns v and
+// Bp = 4/h sum W (v_i - v_c) dpos^T (v_c = 0 unless Pol::kRelativeGradient),
+// the arithmetic of the in-region path.
+template <class T> struct G2POut { T v0, v1, B0, B1, B2, B3; };
+
+template <class Pol>
+__device__ __noinline__ G2POut<typename Pol::real> far_gather(const icy_SimParams &P, const typename Pol::Consts &K,
+                                                              const typename Pol::Node *g, int bx, int by,
+                                                              typename Pol::real fx, typename Pol::real fy,
+                                                              typename Pol::real wx0, typename Pol::real wx1,
+                                                              typename Pol::real wx2, typename Pol::real wy0,
+                                                              typename Pol::real wy1, typename Pol::real wy2,
+                                                              double ind_x, double ind_y)
+{
+    using real = typename Pol::real;
+    const real wx[3] = {wx0, wx1, wx2}, wy[3] = {wy0, wy1, wy2};
+    real vc0 = 0, vc1 = 0;
+    if (Pol::kRelativeGradient) {
+        Pair<real> c = far_node_velocity<Pol>(P, K, g, bx + 1, by + 1, ind_x, ind_y);
+        vc0 = c.a;
+        vc1 = c.b;
+    }
+    G2POut<real> o{0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < 3; i++) {
+        real a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+        for (int j = 0; j < 3; j++) {
+            Pair<real> n = far_node_velocity<Pol>(P, K, g, bx + i, by + j, ind_x, ind_y);
+            const real n0 = n.a - vc0, n1 = n.b - vc1;
+            const real wyd = wy[j] * ((real)j - fy);
+            a0 += wy[j] * n0;
+            a1 += wy[j] * n1;
+            b0 += wyd * n0;
+            b1 += wyd * n1;
+        }
+        const real wxd = wx[i] * ((real)i - fx);
+        o.v0 += wx[i] * a0;
+        o.v1 += wx[i] * a1;
+        o.B0 += wxd * a0;
+        o.B2 += wxd * a1;
+        o.B1 += wx[i] * b0;
+        o.B3 += wx[i] * b1;
+    }
+    const real fhi = Pol::four_h_inv(P, K);
+    o.B0 *= fhi;
+    o.B1 *= fhi;
+    o.B2 *= fhi;
+    o.B3 *= fhi;
+    o.v0 += vc0;  // sum W = 1
+    o.v1 += vc1;
+    return o;
+}
+
+// P2G of a particle whose base node is no longer its binned cell: shared
+// atomics into the warp's region when the stencil lies inside it, global
+// atomics beyond it. Node (i, j) gets W_ij (m, c + S_h (i, j)^T). Returns 1
+// when a stencil node lies outside the grid (the contribution is dropped).
+template <class Pol, int TX, int TY>
+__device__ __noinline__ int stray_p2g(typename Pol::Acc *wacc, int rx0, int ry0, const int GX, const int GY,
+                                      typename Pol::Node *g, uint8_t *dirty, int ntx, int bx, int by,
+                                      typename Pol::real wx0, typename Pol::real wx1, typename Pol::real wx2,
+                                      typename Pol::real wy0, typename Pol::real wy1, typename Pol::real wy2,
+                                      typename Pol::real m, typename Pol::real c0, typename Pol::real c1,
+                                      typename Pol::real S00, typename Pol::real S01, typename Pol::real S10,
+                                      typename Pol::real S11)
+{
+    using real = typename Pol::real;
+    constexpr int RX = TX + 4, RY = TY + 4;
+    const real wx[3] = {wx0, wx1, wx2}, wy[3] = {wy0, wy1, wy2};
+    const int lx = bx - rx0, ly = by - ry0;
+    const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && bx >= 0 && by >= 0 && bx + 2 < GX &&
+                        by + 2 < GY;
+    int bad = 0;
+    for (int i = 0; i < 3; i++) {
+        real cm[3], cx[3], cy[3];
+        const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
+        for (int j = 0; j < 3; j++) {
+            const real W = wx[i] * wy[j];
+            cm[j] = W * m;
+            cx[j] = W * (u0 + S01 * (real)j);
+            cy[j] = W * (u1 + S11 * (real)j);
+        }
+        if (inside) {
+            for (int j = 0; j < 3; j++) {
+                typename Pol::Acc *a = &wacc[(ly + j) * RX + lx + i];
+                real *ap = reinterpret_cast<real *>(a);
+                atomicAdd(ap + acc_off_m(a), cm[j]);
+                atomicAdd(ap + acc_off_x(a), cx[j]);
+                atomicAdd(ap + acc_off_y(a), cy[j]);
+            }
+        } else {
+            bad |= far_scatter<Pol, TX, TY>(GX, GY, g, dirty, ntx, bx + i, by, cm[0], cm[1], cm[2], cx[0], cx[1], cx[2],
+                                            cy[0], cy[1], cy[2]);
+        }
     }
     return bad;
 }
@@ -920,7 +1122,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     int k = 0, r = 0, cur = 0;
     while (k < ng_w && s_wrounds[warp][k] == 0) k++;
     issue(k, 0, 0);
-    real am[9], ax[9], ay[9];
+    CellSums<real> sums;
     while (k < ng_w) {
         int nk, nr;
         next_item(k, r, nk, nr);
@@ -934,10 +1136,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         // a cell whose stencil leaves the grid sends every particle down the
         // stray path, which raises the error word as v2_kernel_p2g does
         const bool cell_ok = cbx + 2 < GX && cby + 2 < GY;
-        if (r == 0) {
-#pragma unroll
-            for (int q = 0; q < 9; q++) { am[q] = 0; ax[q] = 0; ay[q] = 0; }
-        }
+        if (r == 0) sums.zero();
         // P2G of one (updated) particle: node (i, j) gets
         // W_ij (m, c + S_h (i, j)^T) with S = m Bp - dt Vp Dinv tau
         auto p2g = [&](const typename Pol::St &s, const real v0, const real v1, const real *B,
@@ -948,48 +1147,12 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
             const real c0 = v0 * m - (S00 * st.fx + S01 * st.fy);
             const real c1 = v1 * m - (S10 * st.fx + S11 * st.fy);
             if (cell_ok && st.bx == cbx && st.by == cby) {
-#pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
-                    const real wm = st.wx[i] * m;
-#pragma unroll
-                    for (int j = 0; j < 3; j++) {
-                        const real W = st.wx[i] * st.wy[j];
-                        am[i * 3 + j] += wm * st.wy[j];
-                        ax[i * 3 + j] += W * (u0 + S01 * (real)j);
-                        ay[i * 3 + j] += W * (u1 + S11 * (real)j);
-                    }
-                }
+                sums.add(st.wx, st.wy, m, c0, c1, S00, S01, S10, S11);
             } else {
                 stray_count++;
-                const int lx = st.bx - rx0, ly = st.by - ry0;
-                const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 &&
-                                    st.by >= 0 && st.bx + 2 < GX && st.by + 2 < GY;
-#pragma unroll 1
-                for (int i = 0; i < 3; i++) {
-                    real cm[3], cx[3], cy[3];
-                    const real u0 = c0 + S00 * (real)i, u1 = c1 + S10 * (real)i;
-#pragma unroll
-                    for (int j = 0; j < 3; j++) {
-                        const real W = st.wx[i] * st.wy[j];
-                        cm[j] = W * m;
-                        cx[j] = W * (u0 + S01 * (real)j);
-                        cy[j] = W * (u1 + S11 * (real)j);
-                    }
-                    if (inside) {
-#pragma unroll
-                        for (int j = 0; j < 3; j++) {
-                            real *ap = reinterpret_cast<real *>(&wacc[(ly + j) * RX + lx + i]);
-                            atomicAdd(ap + 0, cm[j]);
-                            atomicAdd(ap + 1, cx[j]);
-                            atomicAdd(ap + 2, cy[j]);
-                        }
-                    } else {
-                        bad |= far_scatter<Pol, TX, TY>(GX, GY, gB, R.dirty[R.bufB], R.ntx, st.bx + i, st.by,
-                                                        cm[0], cm[1], cm[2], cx[0], cx[1], cx[2], cy[0], cy[1],
-                                                        cy[2]);
-                    }
-                }
+                bad |= stray_p2g<Pol, TX, TY>(wacc, rx0, ry0, GX, GY, gB, R.dirty[R.bufB], R.ntx, st.bx, st.by,
+                                              st.wx[0], st.wx[1], st.wx[2], st.wy[0], st.wy[1], st.wy[2], m, c0, c1,
+                                              S00, S01, S10, S11);
             }
         };
         // the lane's cell sums into the warp's region: 9 read-modify-write
@@ -1002,12 +1165,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
             for (int i = 0; i < 3; i++)
 #pragma unroll
                 for (int j = 0; j < 3; j++) {
-                    if (cnt > 0 && cell_ok) {
-                        Acc &ac = wacc[ckey + j * RX + i];
-                        Acc v = ac;
-                        acc_add(v, am[i * 3 + j], ax[i * 3 + j], ay[i * 3 + j]);
-                        ac = v;
-                    }
+                    if (cnt > 0 && cell_ok) sums.flush(wacc[ckey + j * RX + i], i, j);
                     __syncwarp();
                 }
         };
@@ -1031,9 +1189,53 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                 const int lx = st.bx - rx0, ly = st.by - ry0;
                 const bool inside = lx >= 0 && ly >= 0 && lx + 2 < RX && ly + 2 < RY && st.bx >= 0 && st.by >= 0 &&
                                     st.bx + 2 < GX && st.by + 2 < GY;
-                real a[3][2], b[3][2];
-                real vc0 = 0, vc1 = 0;  // reference velocity of the relative form
-                if (inside) {
+                if constexpr (sizeof(real) == 4) {
+                    if (inside) {
+                        // the same sums with (x, y) pairs in packed f32x2 arithmetic
+                        const int q0 = ly * RX + lx;
+                        const float2 vc = s_v[q0 + RX + 1];
+                        const float2 nvc = make_float2(-vc.x, -vc.y);
+                        float2 wyy[3], wyd[3], a[3], b[3];
+#pragma unroll
+                        for (int j = 0; j < 3; j++) {
+                            wyy[j] = bcast2(st.wy[j]);
+                            wyd[j] = bcast2(st.wy[j] * ((real)j - st.fy));
+                        }
+#pragma unroll
+                        for (int i = 0; i < 3; i++) {
+                            a[i] = make_float2(0.f, 0.f);
+                            b[i] = make_float2(0.f, 0.f);
+#pragma unroll
+                            for (int j = 0; j < 3; j++) {
+                                const float2 n = __fadd2_rn(s_v[q0 + j * RX + i], nvc);
+                                a[i] = __ffma2_rn(wyy[j], n, a[i]);
+                                b[i] = __ffma2_rn(wyd[j], n, b[i]);
+                            }
+                        }
+                        float2 v = make_float2(0.f, 0.f), b02 = v, b13 = v;
+#pragma unroll
+                        for (int i = 0; i < 3; i++) {
+                            const float2 wxx = bcast2(st.wx[i]), wxd = bcast2(st.wx[i] * ((real)i - st.fx));
+                            v = __ffma2_rn(wxx, a[i], v);
+                            b02 = __ffma2_rn(wxd, a[i], b02);
+                            b13 = __ffma2_rn(wxx, b[i], b13);
+                        }
+                        const float2 f2 = bcast2(fhi);
+                        b02 = __fmul2_rn(b02, f2);
+                        b13 = __fmul2_rn(b13, f2);
+                        v = __fadd2_rn(v, vc);  // sum W = 1
+                        v0 = v.x; v1 = v.y;
+                        B[0] = b02.x; B[1] = b13.x; B[2] = b02.y; B[3] = b13.y;
+                    } else {
+                        const G2POut<real> o = far_gather<Pol>(P, K, gA, st.bx, st.by, st.fx, st.fy, st.wx[0],
+                                                               st.wx[1], st.wx[2], st.wy[0], st.wy[1], st.wy[2],
+                                                               R.ind_x, R.ind_y);
+                        v0 = o.v0; v1 = o.v1;
+                        B[0] = o.B0; B[1] = o.B1; B[2] = o.B2; B[3] = o.B3;
+                    }
+                } else if (inside) {
+                    real a[3][2], b[3][2];
+                    real vc0 = 0, vc1 = 0;  // reference velocity of the relative form
                     const int q0 = ly * RX + lx;
                     if (Pol::kRelativeGradient) {
                         const V2 c = s_v[q0 + RX + 1];
@@ -1054,39 +1256,25 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                             b[i][1] += wyd * n1;
                         }
                     }
-                } else {
-                    if (Pol::kRelativeGradient) {
-                        Pair<real> c = far_node_velocity<Pol>(P, K, gA, st.bx + 1, st.by + 1, R.ind_x, R.ind_y);
-                        vc0 = c.a;
-                        vc1 = c.b;
-                    }
-#pragma unroll 1
-                    for (int i = 0; i < 3; i++) {
-                        a[i][0] = 0; a[i][1] = 0; b[i][0] = 0; b[i][1] = 0;
-                        for (int j = 0; j < 3; j++) {
-                            Pair<real> n = far_node_velocity<Pol>(P, K, gA, st.bx + i, st.by + j, R.ind_x, R.ind_y);
-                            const real n0 = n.a - vc0, n1 = n.b - vc1;
-                            const real wyd = st.wy[j] * ((real)j - st.fy);
-                            a[i][0] += st.wy[j] * n0;
-                            a[i][1] += st.wy[j] * n1;
-                            b[i][0] += wyd * n0;
-                            b[i][1] += wyd * n1;
-                        }
-                    }
-                }
 #pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    const real wxd = st.wx[i] * ((real)i - st.fx);
-                    v0 += st.wx[i] * a[i][0];
-                    v1 += st.wx[i] * a[i][1];
-                    B[0] += wxd * a[i][0];
-                    B[2] += wxd * a[i][1];
-                    B[1] += st.wx[i] * b[i][0];
-                    B[3] += st.wx[i] * b[i][1];
+                    for (int i = 0; i < 3; i++) {
+                        const real wxd = st.wx[i] * ((real)i - st.fx);
+                        v0 += st.wx[i] * a[i][0];
+                        v1 += st.wx[i] * a[i][1];
+                        B[0] += wxd * a[i][0];
+                        B[2] += wxd * a[i][1];
+                        B[1] += st.wx[i] * b[i][0];
+                        B[3] += st.wx[i] * b[i][1];
+                    }
+                    B[0] *= fhi; B[1] *= fhi; B[2] *= fhi; B[3] *= fhi;
+                    v0 += vc0;  // sum W = 1
+                    v1 += vc1;
+                } else {
+                    const G2POut<real> o = far_gather<Pol>(P, K, gA, st.bx, st.by, st.fx, st.fy, st.wx[0], st.wx[1],
+                                                           st.wx[2], st.wy[0], st.wy[1], st.wy[2], R.ind_x, R.ind_y);
+                    v0 = o.v0; v1 = o.v1;
+                    B[0] = o.B0; B[1] = o.B1; B[2] = o.B2; B[3] = o.B3;
                 }
-                B[0] *= fhi; B[1] *= fhi; B[2] *= fhi; B[3] *= fhi;
-                v0 += vc0;  // sum W = 1
-                v1 += vc1;
                 real p_tr, q_tr;
                 int redo;
                 tau = Pol::advance(P, K, s_tab, s, v0, v1, B, p_tr, q_tr, redo);
@@ -1116,8 +1304,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                 // that they are not held across the network's call
                 if (MODE != kModeFinal) {
                     flush_cell_sums();
-#pragma unroll
-                    for (int q = 0; q < 9; q++) { am[q] = 0; ax[q] = 0; ay[q] = 0; }
+                    sums.zero();
                 }
                 Pol::network(K, s_tab, deferred);
                 if (deferred) {
@@ -1184,7 +1371,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
 // earlier launches, heaviest first, which the hardware dispatches first --
 // instead of letting late heavy tiles form the tail of the launch.
 template <class Pol, int TX, int TY, int MODE>
-__global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep(const __grid_constant__ icy_SimParams P,
+__global__ void __maxnreg__(Pol::kMaxRegs) k_tile_substep(const __grid_constant__ icy_SimParams P,
                                                       const __grid_constant__ typename Pol::Consts K,
                                                       const typename Pol::Parts A, const __grid_constant__ TileRun R,
                                                       const __grid_constant__ TmapSet T)
@@ -1254,7 +1441,7 @@ struct EnsLaunch {
 };
 
 template <class Pol, int TX, int TY, int MODE>
-__global__ void __launch_bounds__(256, Pol::kMinBlocks) k_tile_substep_ens(const EnsCase<Pol> *__restrict__ cases,
+__global__ void __maxnreg__(Pol::kMaxRegs) k_tile_substep_ens(const EnsCase<Pol> *__restrict__ cases,
                                                                            const __grid_constant__ EnsLaunch L)
 {
     __shared__ __align__(16) EnsCase<Pol> sc;

@@ -171,19 +171,25 @@ __device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTabl
 }
 
 // FP64 redo of one particle for the cases constitutive32 declines (kept out
-// of line).
-__device__ __noinline__ void constitutive32_via64(const icy_SimParams &P, M2f &H, float &Jp_inv, uint32_t &meta,
-                                                  float &p_tr, float &q_tr)
+// of line). Takes and returns values: state passed by reference to an
+// out-of-line call would have to live in local memory in the caller's hot
+// loop.
+struct Via64 { M2f H; float Jp, p_tr, q_tr; uint32_t meta; };
+
+__device__ __noinline__ Via64 constitutive32_via64(const icy_SimParams &P, const M2f H, const float Jp_inv,
+                                                   const uint32_t meta)
 {
     M2d F = {1.0 + (double)H.a00, (double)H.a01, (double)H.a10, 1.0 + (double)H.a11};
     double jp = Jp_inv, p, q;
     uint8_t cr = (uint8_t)meta32_crushed(meta);
     constitutive64(P, F, jp, cr, meta32_res(meta), p, q);
-    H = {(float)(F.a00 - 1.0), (float)F.a01, (float)F.a10, (float)(F.a11 - 1.0)};
-    Jp_inv = (float)jp;
-    p_tr = (float)p;
-    q_tr = (float)q;
-    meta = (meta & 0x00ffffffu) | ((uint32_t)cr << 24);
+    Via64 o;
+    o.H = {(float)(F.a00 - 1.0), (float)F.a01, (float)F.a10, (float)(F.a11 - 1.0)};
+    o.Jp = (float)jp;
+    o.p_tr = (float)p;
+    o.q_tr = (float)q;
+    o.meta = (meta & 0x00ffffffu) | ((uint32_t)cr << 24);
+    return o;
 }
 
 }  // namespace icm
