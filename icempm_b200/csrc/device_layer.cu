@@ -13,6 +13,7 @@
 // first. Nothing here falls back to the host: every failure is a status.
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled (reached through the runtime, no libcuda link)
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -69,6 +70,7 @@ struct Binning {
     int *key = nullptr, *count = nullptr, *cell_start = nullptr, *cursor = nullptr, *perm = nullptr;
     int *chunk = nullptr, *tile_start = nullptr, *pid = nullptr;
     int *group_slots = nullptr, *group_base = nullptr, *gchunk = nullptr;
+    int *lane_cell = nullptr, *cell_lane = nullptr;  // lane order of the cells of each tile
     size_t cap_pts = 0, cap_cells = 0, cap_tiles = 0, cap_slots = 0;
 };
 
@@ -203,6 +205,17 @@ static Consts32 make_consts32(const icy_SimParams &P)
     k.four_h_inv = (float)(4.0 * P.cellsize_inv);
     k.dt_g = (float)(P.InitialTimeStep * P.Gravity);
     k.vmax = (float)(0.5 * P.cellsize / P.InitialTimeStep);
+    // Wolper_Drucker_Prager (gpu_implementation5.cu:48-94): the hydrostatic
+    // reset's Je_new = sqrt(-2 p_new / kappa + 1) with p_new = -p_thr
+    k.p_thr = (float)P.DP_threshold_p;
+    k.tan_phi = (float)P.DP_tan_phi;
+    k.dp_pmax = (float)P.IceCompressiveStrength;
+    k.dp_qmax = (float)P.IceShearStrength;
+    {
+        const double x = 2.0 * P.DP_threshold_p / P.kappa, je = std::sqrt(x + 1.0);
+        k.je_new = (float)je;
+        k.je_new_m1 = (float)(x / (je + 1.0));
+    }
     // The box p in (-1 MPa, pmax_min / 2), q^2 < inside_q2 lies inside the
     // failure surface of every grain with residues r1 in 0..20, r2 in 0..29,
     // r3 in 0..10 (ids >= 0), by a factor of at least 4 in the terms that
@@ -259,6 +272,7 @@ static void free_binning(icm_ctx *c)
     dfree(c->bin.key); dfree(c->bin.count); dfree(c->bin.cell_start); dfree(c->bin.cursor);
     dfree(c->bin.perm); dfree(c->bin.chunk); dfree(c->bin.tile_start); dfree(c->bin.pid);
     dfree(c->bin.group_slots); dfree(c->bin.group_base); dfree(c->bin.gchunk);
+    dfree(c->bin.lane_cell); dfree(c->bin.cell_lane);
     c->bin = Binning{};
 }
 
@@ -314,7 +328,8 @@ static int ensure_grids(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t
             (rc = dalloc(&c->bin.count, ncells + 1)) || (rc = dalloc(&c->bin.cell_start, ncells + 1)) ||
             (rc = dalloc(&c->bin.cursor, ncells + 1)) || (rc = dalloc(&c->bin.chunk, nchunks + 1)) ||
             (rc = dalloc(&c->bin.tile_start, ntiles + 1)) || (rc = dalloc(&c->bin.group_slots, ngroups + 1)) ||
-            (rc = dalloc(&c->bin.group_base, ngroups + 1)) || (rc = dalloc(&c->bin.gchunk, ngchunks + 1)))
+            (rc = dalloc(&c->bin.group_base, ngroups + 1)) || (rc = dalloc(&c->bin.gchunk, ngchunks + 1)) ||
+            (rc = dalloc(&c->bin.lane_cell, ncells)) || (rc = dalloc(&c->bin.cell_lane, ncells)))
             return rc;
         c->bin.cap_pts = npts;
         c->bin.cap_cells = ncells;
@@ -407,7 +422,10 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
     ICM_LAUNCHED("k_bin_order");
     k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start);
     ICM_LAUNCHED("k_tile_starts");
-    k_group_slots<<<(ngroups + 255) / 256, 256, 0, s>>>(ngroups, c->bin.cell_start, c->bin.group_slots);
+    k_lane_order<<<ntiles, 256, 0, s>>>(g.TX * g.TY, c->bin.cell_start, c->bin.lane_cell, c->bin.cell_lane);
+    ICM_LAUNCHED("k_lane_order");
+    k_group_slots<<<(ngroups + 255) / 256, 256, 0, s>>>(ngroups, c->bin.cell_start, c->bin.lane_cell,
+                                                        c->bin.group_slots);
     ICM_LAUNCHED("k_group_slots");
     if ((rc = scan_ints(c, c->bin.group_slots, ngroups, c->bin.gchunk, c->bin.group_base))) return rc;
     int nslots = 0;
@@ -418,10 +436,12 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
     ICM_CUDA(cudaMemsetAsync(c->bin.pid, 0xff, sizeof(int) * (size_t)std::max(nslots, 1), s));
     if (n > 0) {
         if (storage_form(c->form) == ICM_FORM_FP64)
-            k_pack64<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.key, c->bin.cell_start, c->bin.group_base,
+            k_pack64<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.key, c->bin.cell_start,
+                                                     c->bin.cell_lane, c->bin.group_base,
                                                      c->bin.pid, c->fz.p64);
         else
-            k_pack32<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.key, c->bin.cell_start, c->bin.group_base,
+            k_pack32<<<(n + 255) / 256, 256, 0, s>>>(P, c->bin.perm, c->bin.key, c->bin.cell_start,
+                                                     c->bin.cell_lane, c->bin.group_base,
                                                      c->bin.pid, c->fz.p32);
         ICM_LAUNCHED("k_pack");
     }
@@ -591,7 +611,10 @@ static int rebin_begin(icm_ctx *c, const icy_SimParams &P)
     ICM_LAUNCHED("k_rebin_order");
     k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start);
     ICM_LAUNCHED("k_tile_starts");
-    k_group_slots<<<(ngroups + 255) / 256, 256, 0, s>>>(ngroups, c->bin.cell_start, c->bin.group_slots);
+    k_lane_order<<<ntiles, 256, 0, s>>>(g.TX * g.TY, c->bin.cell_start, c->bin.lane_cell, c->bin.cell_lane);
+    ICM_LAUNCHED("k_lane_order");
+    k_group_slots<<<(ngroups + 255) / 256, 256, 0, s>>>(ngroups, c->bin.cell_start, c->bin.lane_cell,
+                                                        c->bin.group_slots);
     ICM_LAUNCHED("k_group_slots");
     if ((rc = scan_ints(c, c->bin.group_slots, ngroups, c->bin.gchunk, c->bin.group_base))) return rc;
     if (!c->h_ns && cudaMallocHost((void **)&c->h_ns, sizeof(int)) != cudaSuccess) {
@@ -633,11 +656,11 @@ static int rebin_finish(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
     if (n > 0) {
         if (c->fz.form == ICM_FORM_FP64)
             k_rebin_gather<Parts64><<<(n + 255) / 256, 256, 0, s>>>(n, c->bin.perm, c->fz.slot_key, c->bin.cell_start,
-                                                                    c->bin.group_base, c->bin.pid, c->fz.spare_pid,
+                                                                    c->bin.cell_lane, c->bin.group_base, c->bin.pid, c->fz.spare_pid,
                                                                     c->fz.p64, c->fz.s64, keep_pq ? 1 : 0);
         else
             k_rebin_gather<Parts32><<<(n + 255) / 256, 256, 0, s>>>(n, c->bin.perm, c->fz.slot_key, c->bin.cell_start,
-                                                                    c->bin.group_base, c->bin.pid, c->fz.spare_pid,
+                                                                    c->bin.cell_lane, c->bin.group_base, c->bin.pid, c->fz.spare_pid,
                                                                     c->fz.p32, c->fz.s32, keep_pq ? 1 : 0);
         ICM_LAUNCHED("k_rebin_gather");
     }
@@ -791,6 +814,7 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     R.err = c->d_err;
     R.fp64_redo = c->d_redo;
     R.cell_start = c->bin.cell_start;
+    R.lane_cell = c->bin.lane_cell;
     R.group_base = c->bin.group_base;
     R.strays = c->d_strays;
     R.ind_y = p->indenter_y;
@@ -1443,6 +1467,7 @@ int ens_upload_cases(icm_ensemble *e, const std::vector<icy_SimParams> &P, icy_S
         d.R.err = c->d_err;
         d.R.fp64_redo = c->d_redo;
         d.R.cell_start = c->bin.cell_start;
+        d.R.lane_cell = c->bin.lane_cell;
         d.R.group_base = c->bin.group_base;
         d.R.strays = c->d_strays;
         d.R.ind_y = p[i]->indenter_y;

@@ -3,12 +3,14 @@
 // Data layout in HBM (internal, "tile order"):
 //   * particles are binned by their stencil base node (int)(x/h - 0.5); base
 //     nodes (cells) are keyed tile by tile (TX x TY nodes per tile, row-major
-//     inside), and every 32 consecutive keys form a group. Each field is a
-//     structure-of-arrays in ELL slot order: particle r of the cell at lane
-//     L of a group is slot group_base + 32 r + L, with as many rounds as the
-//     group's fullest cell (interior cells of the 4-per-cell lattice hold 4),
-//     so a warp reads one particle of each of its 32 cells per coalesced
-//     vector load;
+//     inside). Inside a tile the cells are put in lane order -- by particle
+//     count, fullest first (lane_cell / cell_lane) -- and every 32
+//     consecutive lanes form a group, so that a group's cells hold similar
+//     counts. Each field is a structure-of-arrays in ELL slot order:
+//     particle r of the cell at lane L of a group is slot
+//     group_base + 32 r + L, with as many rounds as the group's fullest cell
+//     (cells of the 4-per-cell lattice hold 4), so a warp reads one particle
+//     of each of its 32 cells per coalesced vector load;
 //   * the grid is three full-size node buffers G[0..2] of {m, px, py, -};
 //     substep s reads G[s%3] (P2G result of substep s-1), scatters into
 //     G[(s+1)%3] and zeroes G[(s+2)%3] (read by substep s-1), so no separate
@@ -179,7 +181,8 @@ struct TileRun {
     int record_pq;
     unsigned long long *fp64_redo;
     const int *cell_start;          // binning: cell key k holds cell_start[k+1] - cell_start[k] particles
-    const int *group_base;          // first slot of each group of 32 consecutive cell keys
+    const int *lane_cell;           // the cell key at each lane (tile by tile, fullest cells first)
+    const int *group_base;          // first slot of each group of 32 consecutive lanes
     unsigned long long *strays;     // particles that left their binned cell (count)
     // tile scheduling: CTA i runs tile order[i] (tile i when null); a full
     // substep launch writes tile t's clock cycles to cost[t]
@@ -199,6 +202,9 @@ struct TmapSet {
 // 2 an ensemble case scattered outside its active tiles, 4 a tensor copy of
 // a node region did not complete in time
 constexpr int kErrTmaTimeout = 4;
+// bit 8: a cell held more than 65,535 particles (the fused forms' per-cell
+// count field); its particles beyond that were not advanced
+constexpr int kErrCellOverflow = 8;
 
 // launch-order entries of the fused kernel (k_tile_order)
 constexpr int kTileMask = (1 << 29) - 1, kSplitBit = 1 << 29, kHalfBit = 1 << 30;
@@ -362,6 +368,22 @@ struct Pol64 {
         return (P.InitialTimeStep * P.ParticleVolume) * P.Dp_inv;
     }
 };
+
+// Appends a crushed particle's trial state (H, Jp_inv, meta word) to the
+// harvest buffer of the surrogate's training data (out of line: only
+// harvest substeps reach it).
+static __device__ __noinline__ void harvest_state(const Consts32 &k, const M2f H, const float Jp, const uint32_t meta)
+{
+    const unsigned slot = atomicAdd(k.harvest_n, 1u);
+    if (slot >= k.harvest_cap) return;
+    float *h = k.harvest + 6 * (size_t)slot;
+    h[0] = H.a00;
+    h[1] = H.a01;
+    h[2] = H.a10;
+    h[3] = H.a11;
+    h[4] = Jp;
+    h[5] = __uint_as_float(meta);
+}
 
 // FP32 strain form: position = int16 cell + FP32 fraction, H = Fe - I; meta
 // holds the grain's residues and the crushed flag (grain_meta32).
@@ -533,19 +555,11 @@ struct Pol32 {
         p_tr = o.p_tr;
         q_tr = o.q_tr;
     }
-    // the trial state of a crushed particle, for the surrogate's training set
+    // the trial state of a crushed particle, for the surrogate's training
+    // set (only while k.harvest is set)
     static __device__ __forceinline__ void harvest(const Consts &k, const St &s)
     {
-        if (!k.harvest || !meta32_crushed(s.meta)) return;
-        const unsigned slot = atomicAdd(k.harvest_n, 1u);
-        if (slot >= k.harvest_cap) return;
-        float *h = k.harvest + 6 * (size_t)slot;
-        h[0] = s.H.a00;
-        h[1] = s.H.a01;
-        h[2] = s.H.a10;
-        h[3] = s.H.a11;
-        h[4] = s.Jp;
-        h[5] = __uint_as_float(s.meta);
+        if (meta32_crushed(s.meta) && k.harvest) harvest_state(k, s.H, s.Jp, s.meta);
     }
     static __device__ __forceinline__ Tau<float> advance(const icy_SimParams &P, const Consts &k, const Tables &T,
                                                          St &s, float v0, float v1, const float B[4], float &p_tr,
@@ -553,9 +567,9 @@ struct Pol32 {
     {
         advect(k, s, v0, v1, B);
         redo = 0;
+        harvest(k, s);
         Tau32 t;
-        if (constitutive32(k, T, s.H, s.meta, p_tr, q_tr, t) == kC32_NEEDS_FP64) {
-            harvest(k, s);
+        if (constitutive32(k, T, s.H, s.Jp, s.meta, p_tr, q_tr, t) == kC32_NEEDS_FP64) {
             via64(P, s, p_tr, q_tr);
             redo = 1;
             return stress(P, k, s);
@@ -578,55 +592,78 @@ struct Pol32 {
 
 // out-of-line steps of the surrogate form (a crushed particle is rare; the
 // hot loop keeps only the deferred state)
-struct SurrogateOut { M2f H; float Jp, p_tr, q_tr; int accepted; };
+struct SurrogateOut { M2f H; float Jp, p_tr, q_tr; int accepted, fp64; };
 
-// the network's input row (normalised features) of a crushed particle
-// from the FP64 decomposition of its trial state
-static __device__ __noinline__ void surrogate_defer(const icy_SimParams &P, const Consts32 &k, __nv_bfloat16 *row,
-                                                   M2f H, float Jp)
+// The principal stretches s_i - 1 of a trial state from its FP32 invariants:
+// s_i^2 - 1 = e_i = me +- rho, s_i - 1 = e_i / (sqrt(1 + e_i) + 1).
+__device__ __forceinline__ void stretches32(const Inv32 &v, float rho, float &s0m1, float &s1m1)
 {
-    const M2d F = {1.0 + (double)H.a00, (double)H.a01, (double)H.a10, 1.0 + (double)H.a11};
-    const Svd64 d = svd2x2_64(F);
-    float x[kMlpIn];
-    mlp_features(P, d.s0, d.s1, (double)Jp, x);
+    const float e0 = v.me + rho, e1 = v.me - rho;
+    s0m1 = e0 / (sqrtf(1.0f + e0) + 1.0f);
+    s1m1 = e1 / (sqrtf(1.0f + e1) + 1.0f);
+}
+
+// the network's input row (normalised features) of a crushed particle from
+// the FP32 invariants of its trial state; false (nothing written) when
+// det F <= 0.25, which the FP64 form takes
+static __device__ __noinline__ bool surrogate_defer(const Consts32 &k, __nv_bfloat16 *row, const M2f H, const float Jp)
+{
+    const Inv32 v = invariants32(H, k.mu, k.kappa);
+    if (!(v.J > 0.25f)) return false;
+    float s0m1, s1m1;
+    stretches32(v, sqrtf(v.hd * v.hd + v.b01 * v.b01), s0m1, s1m1);
+    const float x[kMlpIn] = {1e3f * s0m1, 1e3f * s1m1, 1e2f * (Jp - 1.0f), k.kappa * 1e-9f, k.tan_phi,
+                             k.dp_qmax * 1e-7f};
 #pragma unroll
     for (int j = 0; j < 8; j++) row[j] = __float2bfloat16(j < kMlpIn ? (x[j] - k.mlp->x_mu[j]) * k.mlp->x_isd[j] : 0.f);
+    return true;
 }
 
 // applies the network's output y (normalised) when it meets the yield
-// condition it stands for, else the exact projection; the decomposition is
-// redone here rather than carried through the round in registers
+// condition it stands for, else the exact projection (dp_map32, FP64 near
+// its discontinuities); all in FP32 strain form from the trial state's
+// invariants, recomputed here rather than carried through the round
 static __device__ __noinline__ SurrogateOut surrogate_finish(const icy_SimParams &P, const Consts32 &k, const float *y,
-                                                             M2f H, float Jp)
+                                                             const M2f H, const float Jp, const uint32_t meta)
 {
-    const M2d F = {1.0 + (double)H.a00, (double)H.a01, (double)H.a10, 1.0 + (double)H.a11};
-    const Svd64 d = svd2x2_64(F);
-    const double s0 = d.s0, s1 = d.s1, jp = Jp;
+    const Inv32 v = invariants32(H, k.mu, k.kappa);
+    const float rho = sqrtf(v.hd * v.hd + v.b01 * v.b01);
+    float s0m1, s1m1;
+    stretches32(v, rho, s0m1, s1m1);
+    const float s0 = 1.0f + s0m1, s1 = 1.0f + s1m1;
     // p and q of the trial state (ComputePQ, gpu_implementation5.cu:36-44)
-    const double Je = s0 * s1, ptr = -(P.kappa / 2.) * (Je * Je - 1.);
-    const double sq0 = s0 * s0, sq1 = s1 * s1, qtr = P.mu / Je * fabs(sq0 - sq1);
-    const double s0n = s0 + 1e-3 * (double)(y[0] * k.mlp->y_sd[0] + k.mlp->y_mu[0]);
-    const double s1n = s1 + 1e-3 * (double)(y[1] * k.mlp->y_sd[1] + k.mlp->y_mu[1]);
-    const double tol = k.mlp_tol, p_thr = P.DP_threshold_p;
-    DpResult r{false, s0, s1, jp};
-    bool ok = false;
-    if (!(ptr < -p_thr || jp < 1) && isfinite(s0n) && isfinite(s1n) && s0n > 0 && s1n > 0) {
-        const double q_n_1 =
-            (ptr > P.IceCompressiveStrength) ? 0.0 : fmin((ptr + p_thr) * P.DP_tan_phi, P.IceShearStrength);
-        if (qtr >= q_n_1) {
-            const double sq0n = s0n * s0n, sq1n = s1n * s1n, qn = P.mu / (s0n * s1n) * fabs(sq0n - sq1n);
-            ok = fabs(qn - q_n_1) <= tol * P.IceShearStrength && fabs((sq0n + sq1n) - (sq0 + sq1)) <= tol * 1e-3;
-            r = {true, s0n, s1n, jp};
+    const float p = -0.5f * v.s2, q = 2.0f * v.s1 * rho;
+    const float ds0 = 1e-3f * (y[0] * k.mlp->y_sd[0] + k.mlp->y_mu[0]);
+    const float ds1 = 1e-3f * (y[1] * k.mlp->y_sd[1] + k.mlp->y_mu[1]);
+    const float tol = k.mlp_tol;
+    SurrogateOut o{H, Jp, p, q, 0, 0};
+    bool ok = false, moved = false;
+    if (!(p < -k.p_thr || Jp < 1.0f) && isfinite(ds0) && isfinite(ds1) && s0 + ds0 > 0.0f && s1 + ds1 > 0.0f) {
+        const float qn = (p > k.dp_pmax) ? 0.0f : fminf((p + k.p_thr) * k.tan_phi, k.dp_qmax);
+        if (q >= qn) {
+            // q of the predicted stretches: mu/(s0' s1') (s0' - s1')(s0' + s1')
+            const float s0n = s0 + ds0, s1n = s1 + ds1;
+            const float gap = 2.0f * rho / (s0 + s1) + (ds0 - ds1);
+            const float qp = k.mu / (s0n * s1n) * fabsf(gap * (s0n + s1n));
+            const float dsum = ds0 * (2.0f * s0 + ds0) + ds1 * (2.0f * s1 + ds1);  // change of s0^2 + s1^2
+            ok = fabsf(qp - qn) <= tol * k.dp_qmax && fabsf(dsum) <= tol * 1e-3f;
+            moved = ok;
         } else {
-            ok = fabs(s0n - s0) <= tol * 1e-3 && fabs(s1n - s1) <= tol * 1e-3;
+            ok = fabsf(ds0) <= tol * 1e-3f && fabsf(ds1) <= tol * 1e-3f;
         }
     }
-    if (!ok) r = dp_project64(P, s0, s1, jp);
-    SurrogateOut o{H, Jp, (float)ptr, (float)qtr, ok ? 1 : 0};
-    if (r.changed) {
-        const M2d Fe = usvt64(d, r.s0, r.s1);
-        o.H = {(float)(Fe.a00 - 1.0), (float)Fe.a01, (float)Fe.a10, (float)(Fe.a11 - 1.0)};
-        o.Jp = (float)r.jp;
+    if (ok) {
+        if (moved) scale_principal32(o.H, v, rho, ds0 / s0, ds1 / s1);
+        o.accepted = 1;
+        return o;
+    }
+    if (!(v.J > 0.25f) || dp_map32(k, o.H, o.Jp, v, p, q, rho) != kC32_OK) {
+        const Via64 r = constitutive32_via64(P, H, Jp, meta);
+        o.H = r.H;
+        o.Jp = r.Jp;
+        o.p_tr = r.p_tr;
+        o.q_tr = r.q_tr;
+        o.fp64 = 1;
     }
     return o;
 }
@@ -687,16 +724,17 @@ struct Pol32S : Pol32 {
     {
         advect(k, s, v0, v1, B);
         redo = 0;
-        Tau32 t;
-        if (constitutive32(k, T, s.H, s.meta, p_tr, q_tr, t) == kC32_OK) return {t.t00, t.t01, t.t01, t.t11};
         harvest(k, s);
-        if (k.mlp && meta32_crushed(s.meta)) {
-            surrogate_defer(P, k,
-                            reinterpret_cast<__nv_bfloat16 *>(T.rows[threadIdx.x >> 5] + (threadIdx.x & 31) * 16),
-                            s.H, s.Jp);
+        // a crushed particle's projection is the network's (from the FP32
+        // invariants; det F <= 0.25 goes to the FP64 form)
+        if (k.mlp && meta32_crushed(s.meta) &&
+            surrogate_defer(k, reinterpret_cast<__nv_bfloat16 *>(T.rows[threadIdx.x >> 5] + (threadIdx.x & 31) * 16),
+                            s.H, s.Jp)) {
             redo = 2;
             return {0.f, 0.f, 0.f, 0.f};
         }
+        Tau32 t;
+        if (constitutive32(k, T, s.H, s.Jp, s.meta, p_tr, q_tr, t) == kC32_OK) return {t.t00, t.t01, t.t01, t.t11};
         via64(P, s, p_tr, q_tr);
         redo = 1;
         return stress(P, k, s);
@@ -710,17 +748,18 @@ struct Pol32S : Pol32 {
     }
     static __device__ __forceinline__ Tau<float> finish(const icy_SimParams &P, const Consts &k, const Tables &T,
                                                         St &s, float &p_tr, float &q_tr, unsigned &accepted,
-                                                        unsigned &exact)
+                                                        unsigned &exact, unsigned &fp64)
     {
         const SurrogateOut o =
             surrogate_finish(P, k, reinterpret_cast<const float *>(T.rows[threadIdx.x >> 5] + (threadIdx.x & 31) * 16),
-                             s.H, s.Jp);
+                             s.H, s.Jp, s.meta);
         s.H = o.H;
         s.Jp = o.Jp;
         p_tr = o.p_tr;
         q_tr = o.q_tr;
         accepted += o.accepted;
         exact += 1 - o.accepted;
+        fp64 += o.fp64;
         return stress(P, k, s);
     }
 };
@@ -877,6 +916,17 @@ __device__ __noinline__ int stray_p2g(typename Pol::Acc *wacc, int rx0, int ry0,
     return bad;
 }
 
+// The j-th group a warp takes: warps take groups in a snake order (w, then
+// 2 nwarps - 1 - w, ...) so that the fullest groups, which come first, are
+// spread over the warps; the halves of a split tile (part 1, 2) take the
+// even and the odd groups. Returns a value >= the tile's group count when
+// the warp has no j-th group.
+__device__ __forceinline__ int group_of(int j, int warp, int nwarps, int part)
+{
+    const int m = j * nwarps + ((j & 1) ? nwarps - 1 - warp : warp);
+    return part == 0 ? m : 2 * m + (part - 1);
+}
+
 // Dynamic shared memory of one CTA (host and kernel use the same layout):
 // the warps' P2G regions (none in the final launch), then two staging rounds
 // per warp.
@@ -913,7 +963,9 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     __shared__ double s_tot[2];
     __shared__ int s_contact, s_mark[9];
     __shared__ typename Pol::Tables s_tab;
-    __shared__ int s_wcnt[kMaxWarps][kMaxGroupsPerWarp][32];
+    // per lane of each of the warp's groups: its cell inside the tile
+    // (bits 16-31) and the cell's particle count (bits 0-15)
+    __shared__ uint32_t s_wcnt[kMaxWarps][kMaxGroupsPerWarp][32];
     __shared__ int s_wrounds[kMaxWarps][kMaxGroupsPerWarp], s_wgbase[kMaxWarps][kMaxGroupsPerWarp];
 
     const int tx = t % R.ntx, ty = t / R.ntx;
@@ -927,23 +979,26 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     const unsigned FULL = 0xffffffffu;
     const int lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
     constexpr int CELLS = TX * TY;
-    // part 0: the whole tile; parts 1 and 2: the first and second half of
-    // the tile's cell groups (a heavy tile split over two CTAs). Both halves
+    // part 0: the whole tile; parts 1 and 2: the even and the odd cell
+    // groups of the tile (a heavy tile split over two CTAs). Both halves
     // update the node region; the first owns the tile's zeroing and its
     // reaction force.
     const int NGT_ = TX * TY / 32;
-    const int g_lo = part == 2 ? NGT_ / 2 : 0, g_hi = part == 1 ? NGT_ / 2 : NGT_;
     // What depends only on the binning (unchanged since the last re-binning
     // or pack, both finished before this launch could start) is set up
-    // before the wait for the previous substep: this warp's groups g = warp,
-    // warp + nwarps, ... (at most kMaxGroupsPerWarp) with their cell counts,
-    // rounds and slot bases, and the grain tables.
+    // before the wait for the previous substep: this warp's groups
+    // (group_of, at most kMaxGroupsPerWarp) with their lanes' cells, cell
+    // counts, rounds and slot bases, and the grain tables.
     int ng_w = 0;
     if (p1 > p0) {
-        for (int g = g_lo + warp; g < g_hi; g += nwarps, ng_w++) {
-            const int c = t * CELLS + g * 32 + lane;
-            const int cnt = R.cell_start[c + 1] - R.cell_start[c];
-            s_wcnt[warp][ng_w][lane] = cnt;
+        for (int g; (g = group_of(ng_w, warp, nwarps, part)) < NGT_; ng_w++) {
+            const int c = R.lane_cell[t * CELLS + g * 32 + lane];
+            int cnt = R.cell_start[c + 1] - R.cell_start[c];
+            if (cnt > 0xffff) {  // beyond the count field: the cell's later particles are not advanced
+                atomicOr(R.err, kErrCellOverflow);
+                cnt = 0xffff;
+            }
+            s_wcnt[warp][ng_w][lane] = ((uint32_t)(c - t * CELLS) << 16) | (uint32_t)cnt;
             const int rounds = __reduce_max_sync(FULL, cnt);
             if (lane == 0) {
                 s_wrounds[warp][ng_w] = rounds;
@@ -1116,7 +1171,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         }
     };
     auto issue = [&](int k, int r, int st) {
-        if (k < ng_w && r < s_wcnt[warp][k][lane]) Pol::prefetch(A, s_wgbase[warp][k] + 32 * r + lane, stage[st], lane);
+        if (k < ng_w && r < (int)(s_wcnt[warp][k][lane] & 0xffffu)) Pol::prefetch(A, s_wgbase[warp][k] + 32 * r + lane, stage[st], lane);
         __pipeline_commit();
     };
     int k = 0, r = 0, cur = 0;
@@ -1128,11 +1183,11 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         next_item(k, r, nk, nr);
         issue(nk, nr, cur ^ 1);
         __pipeline_wait_prior(1);
-        const int g = g_lo + warp + k * nwarps;
-        const int cl = g * 32 + lane;
+        const uint32_t wc = s_wcnt[warp][k][lane];
+        const int cl = (int)(wc >> 16);
         const int clx = cl % TX, cly = cl / TX;
         const int cbx = x0 + clx, cby = y0 + cly;  // the cell's base node
-        const int cnt = s_wcnt[warp][k][lane];
+        const int cnt = (int)(wc & 0xffffu);
         // a cell whose stencil leaves the grid sends every particle down the
         // stray path, which raises the error word as v2_kernel_p2g does
         const bool cell_ok = cbx + 2 < GX && cby + 2 < GY;
@@ -1314,8 +1369,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
                     uint32_t dmeta;
                     Pol::defer_load(s_tab, A, dp, ds, dv0, dv1, dB, djp, dmeta);
                     real p_tr, q_tr;
-                    const Tau<real> t2 = Pol::finish(P, K, s_tab, ds, p_tr, q_tr, mlp_ok, mlp_fb);
-                    redo_count += 1;
+                    const Tau<real> t2 = Pol::finish(P, K, s_tab, ds, p_tr, q_tr, mlp_ok, mlp_fb, redo_count);
                     Pol::store(A, dp, ds, djp, dmeta);
                     if (R.record_pq) A.pq[dp] = {p_tr, q_tr};
                     if (MODE == kModeFinal) {
@@ -1714,22 +1768,71 @@ __global__ void k_bin_order(int ncells, const int *start, int *perm)
     }
 }
 
-// Slots of each group of 32 consecutive cell keys: 32 x the largest count.
-__global__ void k_group_slots(int ngroups, const int *cell_start, int *group_slots)
+// Lane order of the cells of each tile (one CTA per tile, cells_per_tile a
+// power of two <= kMaxTileCells): by particle count, fullest first, ties by
+// cell key. lane_cell[l] is the cell key at lane l and cell_lane its inverse;
+// both index the tile's own range of keys, t * cells_per_tile + i. A group
+// of 32 consecutive lanes then holds cells of similar counts, so that few of
+// its lanes idle through the rounds of its fullest cell.
+constexpr int kMaxTileCells = 512;
+
+__global__ void __launch_bounds__(256) k_lane_order(int cells_per_tile, const int *cell_start, int *lane_cell,
+                                                    int *cell_lane)
+{
+    __shared__ uint32_t s_key[kMaxTileCells];
+    const int base = blockIdx.x * cells_per_tile, n = cells_per_tile;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int cnt = min(cell_start[base + i + 1] - cell_start[base + i], 0xffff);
+        s_key[i] = ((uint32_t)(0xffff - cnt) << 16) | (uint32_t)i;  // ascending key = descending count
+    }
+    __syncthreads();
+    for (int k = 2; k <= n; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const uint32_t a = s_key[i], b = s_key[l];
+                    if (((i & k) == 0) ? (a > b) : (a < b)) {
+                        s_key[i] = b;
+                        s_key[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int cell = (int)(s_key[i] & 0xffffu);
+        lane_cell[base + i] = base + cell;
+        cell_lane[base + cell] = base + i;
+    }
+}
+
+// Slots of each group of 32 consecutive lanes: 32 x the largest count.
+__global__ void k_group_slots(int ngroups, const int *cell_start, const int *lane_cell, int *group_slots)
 {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= ngroups) return;
     int mx = 0;
-    for (int l = 0; l < 32; l++) mx = max(mx, cell_start[g * 32 + l + 1] - cell_start[g * 32 + l]);
+    for (int l = 0; l < 32; l++) {
+        const int c = lane_cell[g * 32 + l];
+        mx = max(mx, cell_start[c + 1] - cell_start[c]);
+    }
     group_slots[g] = 32 * mx;
+}
+
+// Slot of particle r of the cell with key k.
+__device__ __forceinline__ int slot_in_cell(int k, int r, const int *cell_lane, const int *group_base)
+{
+    const int l = cell_lane[k];
+    return group_base[l >> 5] + 32 * r + (l & 31);
 }
 
 // Slot of the particle at sorted position q (perm order = key order).
 __device__ __forceinline__ int slot_of(int q, const int *perm, const int *key, const int *cell_start,
-                                       const int *group_base)
+                                       const int *cell_lane, const int *group_base)
 {
-    int k = key[perm[q]];
-    return group_base[k >> 5] + 32 * (q - cell_start[k]) + (k & 31);
+    const int k = key[perm[q]];
+    return slot_in_cell(k, q - cell_start[k], cell_lane, group_base);
 }
 
 __global__ void k_tile_starts(int ntiles, int cells_per_tile, const int *cell_start, int *tile_start)
@@ -1746,12 +1849,12 @@ __device__ __forceinline__ uint32_t read_meta(const icy_SimParams &P, int i)
 }
 
 __global__ void k_pack64(const icy_SimParams P, const int *perm, const int *key, const int *cell_start,
-                         const int *group_base, int *pid, Parts64 A)
+                         const int *cell_lane, const int *group_base, int *pid, Parts64 A)
 {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.nPts) return;
     int i = perm[q];
-    int k = slot_of(q, perm, key, cell_start, group_base);
+    int k = slot_of(q, perm, key, cell_start, cell_lane, group_base);
     const double *pts = P.pts_array;
     const size_t pp = P.nPtsPitch;
     auto row = [&](int r) { return pts[(size_t)r * pp + i]; };
@@ -1789,12 +1892,12 @@ __global__ void k_unpack64(const icy_SimParams P, int nslots, const int *pid, co
 }
 
 __global__ void k_pack32(const icy_SimParams P, const int *perm, const int *key, const int *cell_start,
-                         const int *group_base, int *pid, Parts32 A)
+                         const int *cell_lane, const int *group_base, int *pid, Parts32 A)
 {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= P.nPts) return;
     int i = perm[q];
-    int k = slot_of(q, perm, key, cell_start, group_base);
+    int k = slot_of(q, perm, key, cell_start, cell_lane, group_base);
     const double *pts = P.pts_array;
     const size_t pp = P.nPtsPitch;
     auto row = [&](int r) { return pts[(size_t)r * pp + i]; };
@@ -1923,14 +2026,14 @@ __device__ __forceinline__ void copy_slot(const Parts64 &S, int from, const Part
 
 template <class Parts>
 __global__ void k_rebin_gather(int n, const int *order, const int *slot_key, const int *cell_start,
-                               const int *group_base, const int *pid_old, int *pid_new, const Parts S, const Parts D,
-                               int pq)
+                               const int *cell_lane, const int *group_base, const int *pid_old, int *pid_new,
+                               const Parts S, const Parts D, int pq)
 {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
     int old = order[q];
     int k = slot_key[old];
-    int ns = group_base[k >> 5] + 32 * (q - cell_start[k]) + (k & 31);
+    int ns = slot_in_cell(k, q - cell_start[k], cell_lane, group_base);
     copy_slot(S, old, D, ns, pq != 0);
     pid_new[ns] = pid_old[old];
 }

@@ -7,7 +7,8 @@
 //
 // Invariants, shared by the Kirchhoff stress and the failure check:
 //   J - 1 = tr H + det H,  b - I = F F^T - I = H + H^T + H H^T,
-//   hd = ((b - I)_00 - (b - I)_11)/2,  b01 = (b - I)_01.
+//   hd = ((b - I)_00 - (b - I)_11)/2,  b01 = (b - I)_01,
+//   me = ((b - I)_00 + (b - I)_11)/2.
 // Kirchhoff stress (gpu_implementation5.cu:24-34):
 //   tau = s1 dev(b) + s2 I with s1 = mu/J, s2 = kappa (J^2 - 1).
 // ComputePQ (gpu_implementation5.cu:36-44) needs no SVD for p and q: the
@@ -16,15 +17,12 @@
 //   q = sqrt(2) |mu/J dev(sigma^2)| = (mu/J)(sigma0^2 - sigma1^2)
 //     = 2 s1 sqrt(hd^2 + b01^2).
 // An intact particle whose (p, q) is clearly inside its failure surface is
-// done here in FP32. Everything else -- the crush decision at the surface,
-// every crushed particle (SVD + Drucker-Prager map, gpu_implementation5.cu:
-// 48-94, helper_math.cuh:27-140) and ill-conditioned states (det F small or
-// negative) -- is redone in FP64 with the reference form (mpm_math64.cuh).
-// Crushed particles are a fraction of a percent of a block and sit together
-// near the indenter, so this costs no measurable time; it is done for all of
-// them, not only for nearly equal singular values, because the indentation's
-// crushing outcome is sensitive to strain perturbations of a few 1e-8 and an
-// FP32 return map moved the peak indenter force of a 10k-substep run by ~4%.
+// done here in FP32, and so is the Drucker-Prager map of a crushed particle
+// (dp_map32: in strain form, from the same invariants, no SVD). The rest --
+// the crush decision at the failure surface, a crushed particle within a
+// relative 1e-4 of a discontinuity of the map, and ill-conditioned states
+// (det F small or negative) -- is redone in FP64 with the reference form
+// (mpm_math64.cuh).
 #pragma once
 #include <cstdint>
 #include "mpm_math64.cuh"
@@ -41,6 +39,10 @@ struct Consts32 {
     float gv, ics, its, iss;                        // grain variability, strengths in MPa
     float four_h_inv;
     float dt_g, vmax;                               // dt*gravity, 0.5 h/dt
+    // Drucker-Prager map (Pa): threshold pressure, tan(phi), the
+    // compressive and shear strengths it uses (not grain-varied), Je of the
+    // hydrostatic reset sqrt(1 + 2 p_thr/kappa) and Je - 1
+    float p_thr, tan_phi, dp_pmax, dp_qmax, je_new, je_new_m1;
     // a box in (p, q) (MPa) inside every failure surface that a grain with a
     // non-negative id can have, with a wide margin: a particle of such a
     // grain inside it needs no table lookup to be found intact (q2 = 0: none)
@@ -86,20 +88,29 @@ __device__ __forceinline__ GrainRes meta32_res(uint32_t m)
     return {(int)(m & 63u) - 20, (int)((m >> 6) & 63u) - 29, (int)((m >> 12) & 31u) - 10};
 }
 
-// Stress and (p, q) of one H.
-struct Inv32 { float J, s1, s2, hd, b01; };
+// Stress and (p, q) of one H: J = det F, s1 = mu/J, s2 = kappa (J^2 - 1),
+// and b - I = me I + [[hd, b01], [b01, -hd]] (eigenvalues me +- |(hd, b01)|,
+// the squared singular values of F minus one).
+struct Inv32 { float J, Jm1, s1, s2, hd, b01, me; };
 
-__device__ __forceinline__ Inv32 invariants32(const M2f &H, float mu, float kappa)
+__host__ __device__ __forceinline__ Inv32 invariants32(const M2f &H, float mu, float kappa)
 {
     Inv32 v;
-    float Jm1 = (H.a00 + H.a11) + (H.a00 * H.a11 - H.a01 * H.a10);
-    v.J = 1.0f + Jm1;
+    v.Jm1 = (H.a00 + H.a11) + (H.a00 * H.a11 - H.a01 * H.a10);
+    v.J = 1.0f + v.Jm1;
     float b00 = 2.0f * H.a00 + H.a00 * H.a00 + H.a01 * H.a01;
     float b11 = 2.0f * H.a11 + H.a10 * H.a10 + H.a11 * H.a11;
     v.b01 = H.a01 + H.a10 + H.a00 * H.a10 + H.a01 * H.a11;
-    v.hd = 0.5f * (b00 - b11);
+    // (b00 - b11)/2 factored so that a mostly volumetric strain (b00 ~ b11)
+    // does not cancel: (H00 - H11)(1 + (H00 + H11)/2) + (H01 - H10)(H01 + H10)/2
+    v.hd = (H.a00 - H.a11) * (1.0f + 0.5f * (H.a00 + H.a11)) + 0.5f * (H.a01 - H.a10) * (H.a01 + H.a10);
+    v.me = 0.5f * (b00 + b11);
+#ifdef __CUDA_ARCH__
     v.s1 = __fdividef(mu, v.J);
-    v.s2 = kappa * Jm1 * (v.J + 1.0f);
+#else
+    v.s1 = mu / v.J;
+#endif
+    v.s2 = kappa * v.Jm1 * (v.J + 1.0f);
     return v;
 }
 
@@ -144,20 +155,111 @@ __device__ __forceinline__ int failure_side32(const GrainTables32 &T, uint32_t m
     return a + b > 0.0f ? 1 : 0;
 }
 
-// Result codes of constitutive32.
+// Result codes of constitutive32 and dp_map32.
 enum { kC32_OK = 0, kC32_NEEDS_FP64 = 1 };
 
-// ComputePQ + failure check of an intact particle whose (p, q) lies clearly
-// inside its failure surface: the state is unchanged, tau is the Kirchhoff
-// stress of H. Returns kC32_NEEDS_FP64 (state untouched) for a crushed
-// particle, for one on or outside the surface or within kSurfaceMargin of
-// it, and for det F <= 0.25.
-__device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTables32 &T, const M2f &H, uint32_t meta,
-                                              float &p_tr, float &q_tr, Tau32 &tau)
+// Relative distance from a discontinuity of the Drucker-Prager map (the
+// hydrostatic threshold p = -p_thr, the compressive strength p = pmax)
+// inside which the FP32 form redoes the map in FP64.
+constexpr float kDpMargin = 1e-4f;
+
+// Wolper_Drucker_Prager (gpu_implementation5.cu:48-94) of a crushed
+// particle in strain form, without an SVD. With F = U S V^T and
+// b = F F^T = U S^2 U^T, the map keeps U and V and replaces the singular
+// values, so F_new = U diag(r) U^T F with r_i = s_new_i / s_i, and
+//   H_new = F_new - I = (M - I) + (M - I) H + H,
+//   M - I = U diag(r - 1) U^T = a I + c [[hd, b01], [b01, -hd]] / rho,
+// a = (r0 - 1 + r1 - 1)/2, c = (r0 - r1)/2, rho = |(hd, b01)| (U's first
+// column is b's eigenvector of the larger eigenvalue me + rho). Every term
+// is formed from small quantities (strains), so FP32 keeps their relative
+// accuracy:
+// * hydrostatic branch (p < -p_thr or Jp_inv < 1): s_new_i^2 = Je_new, so
+//   r_i^2 - 1 = (Je_new - 1 - e_i)/(1 + e_i) with e_i = me +- rho, and
+//   Jp_inv *= Je_new / J;
+// * cone (q >= q_n+1): the mean of s^2 is kept and its half-gap rho becomes
+//   rho q_n+1 / q, so e_new_i - e_i = +-(rho_new - rho) and
+//   r_i^2 - 1 = (e_new_i - e_i)/(1 + e_i);
+// * inside the cone: unchanged.
+// r_i - 1 = (r_i^2 - 1)/(sqrt(r_i^2) + 1) avoids the cancellation of
+// sqrt(.) - 1. p and q are the trial state's (p = -s2/2, q = 2 s1 rho).
+// Returns kC32_NEEDS_FP64 (state untouched) within kDpMargin of the map's
+// discontinuities, where float rounding could select another branch than
+// the FP64 form would.
+// F_new = U diag(r) U^T F in strain form, given r_i - 1 (U: eigenvectors of
+// b = F F^T, the first for the larger eigenvalue).
+__host__ __device__ __forceinline__ void scale_principal32(M2f &H, const Inv32 &v, float rho, float r0m1, float r1m1)
+{
+    const float a = 0.5f * (r0m1 + r1m1), c = 0.5f * (r0m1 - r1m1);
+    const float cn = rho > 0.0f ? c / rho : 0.0f;  // c = 0 whenever rho = 0
+    const float m00 = a + cn * v.hd, m01 = cn * v.b01, m11 = a - cn * v.hd;
+    const M2f h = H;
+    H.a00 = h.a00 + (m00 + (m00 * h.a00 + m01 * h.a10));
+    H.a01 = h.a01 + (m01 + (m00 * h.a01 + m01 * h.a11));
+    H.a10 = h.a10 + (m01 + (m01 * h.a00 + m11 * h.a10));
+    H.a11 = h.a11 + (m11 + (m01 * h.a01 + m11 * h.a11));
+}
+
+__host__ __device__ __forceinline__ int dp_map32(const Consts32 &k, M2f &H, float &Jp_inv, const Inv32 &v, float p,
+                                                 float q, float rho)
+{
+    if (fabsf(p + k.p_thr) <= kDpMargin * fmaxf(k.p_thr, fabsf(p)) || fabsf(p - k.dp_pmax) <= kDpMargin * k.dp_pmax)
+        return kC32_NEEDS_FP64;
+    const float e0 = v.me + rho, e1 = v.me - rho;
+    float d0, d1;  // r_i^2 - 1
+    if (p < -k.p_thr || Jp_inv < 1.0f) {
+        d0 = (k.je_new_m1 - e0) / (1.0f + e0);
+        d1 = (k.je_new_m1 - e1) / (1.0f + e1);
+        Jp_inv *= k.je_new / v.J;
+    } else {
+        const float qn = (p > k.dp_pmax) ? 0.0f : fminf((p + k.p_thr) * k.tan_phi, k.dp_qmax);
+        if (!(q >= qn) || !(q > 0.0f)) return kC32_OK;
+        const float drho = -rho * ((q - qn) / q);  // rho_new - rho
+        d0 = drho / (1.0f + e0);
+        d1 = -drho / (1.0f + e1);
+    }
+    scale_principal32(H, v, rho, d0 / (sqrtf(1.0f + d0) + 1.0f), d1 / (sqrtf(1.0f + d1) + 1.0f));
+    return kC32_OK;
+}
+
+// ComputePQ and dp_map32 of a crushed particle (kept out of line: crushed
+// particles are few, and the map's values would add to the register
+// pressure of every particle's update). tau is the Kirchhoff stress of the
+// new H; rc is dp_map32's.
+struct Crushed32 { M2f H; float Jp, p, q; Tau32 tau; int rc; };
+
+__device__ __noinline__ Crushed32 crushed32(const Consts32 &k, const M2f H, const float Jp)
+{
+    Crushed32 o{H, Jp, 0.0f, 0.0f, {0.0f, 0.0f, 0.0f}, kC32_OK};
+    const Inv32 v = invariants32(H, k.mu, k.kappa);
+    const float rho = sqrtf(v.hd * v.hd + v.b01 * v.b01);
+    o.p = -0.5f * v.s2;
+    o.q = 2.0f * v.s1 * rho;
+    o.rc = dp_map32(k, o.H, o.Jp, v, o.p, o.q, rho);
+    if (o.rc == kC32_OK) o.tau = tau32(invariants32(o.H, k.mu, k.kappa));
+    return o;
+}
+
+// ComputePQ, then for an intact particle the failure check, for a crushed
+// one the Drucker-Prager map (dp_map32); tau is the Kirchhoff stress of the
+// new H. Returns kC32_NEEDS_FP64 (state untouched) for an intact particle on
+// or outside its failure surface or within kSurfaceMargin of it, for a
+// crushed one near a discontinuity of the map, and for det F <= 0.25.
+__device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTables32 &T, M2f &H, float &Jp_inv,
+                                              uint32_t meta, float &p_tr, float &q_tr, Tau32 &tau)
 {
     Inv32 v = invariants32(H, k.mu, k.kappa);
-    if (!(v.J > 0.25f) || meta32_crushed(meta)) return kC32_NEEDS_FP64;
-    float p = -0.5f * v.s2;
+    if (!(v.J > 0.25f)) return kC32_NEEDS_FP64;
+    const float p = -0.5f * v.s2;
+    if (meta32_crushed(meta)) {
+        const Crushed32 o = crushed32(k, H, Jp_inv);
+        if (o.rc != kC32_OK) return kC32_NEEDS_FP64;
+        H = o.H;
+        Jp_inv = o.Jp;
+        p_tr = o.p;
+        q_tr = o.q;
+        tau = o.tau;
+        return kC32_OK;
+    }
     float q = 2.0f * v.s1 * approx_sqrt(v.hd * v.hd + v.b01 * v.b01);
     // residues at or above their offsets: the grain id is not negative
     const bool grain_nonneg = (meta & 63u) >= 20u && ((meta >> 6) & 63u) >= 29u && ((meta >> 12) & 31u) >= 10u;
