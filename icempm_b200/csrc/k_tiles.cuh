@@ -266,6 +266,10 @@ struct Pol64 {
     static constexpr bool kHarvest = false;  // Consts has no harvest fields
     // registers per thread: three 128-thread CTAs per SM
     static constexpr int kMaxRegs = 168;
+    // staging rounds per warp (the particle state of a round is copied into
+    // shared memory kStages - 1 rounds ahead); three would cost the FP64
+    // form its third CTA per SM
+    static constexpr int kStages = 2;
     // Bp from raw node velocities, operation order of the reference
     static constexpr bool kRelativeGradient = false;
     using real = double;
@@ -392,6 +396,9 @@ struct Pol32 {
     static constexpr bool kHarvest = true;
     // registers per thread: four 128-thread CTAs per SM
     static constexpr int kMaxRegs = 128;
+    // staging rounds per warp (the particle state of a round is copied into
+    // shared memory kStages - 1 rounds ahead)
+    static constexpr int kStages = 2;
     // Bp = 4/h sum W (v_i - v_c) dpos^T with v_c the stencil's centre node:
     // equal to the reference's sum since sum W dpos = 0, but free of the
     // cancellation of a large common velocity (whose FP32 residual would
@@ -680,6 +687,9 @@ static __device__ __noinline__ SurrogateOut surrogate_finish(const icy_SimParams
 // Jp_inv < 1, a closed form with nothing to learn), the exact map runs.
 struct Pol32S : Pol32 {
     static constexpr bool kSurrogate = true;
+    // two staging rounds: a third would not leave room for four CTAs per SM
+    // next to the network's rows
+    static constexpr int kStages = 2;
     // at most kWarps warps per CTA (128 threads) in this form
     static constexpr int kWarps = 4;
     // A particle held back for the network: slot, state after advection,
@@ -928,17 +938,24 @@ __device__ __forceinline__ int group_of(int j, int warp, int nwarps, int part)
 }
 
 // Dynamic shared memory of one CTA (host and kernel use the same layout):
-// the warps' P2G regions (none in the final launch), then two staging rounds
-// per warp.
+// the warps' P2G regions (none in the final launch), then Pol::kStages
+// staging rounds per warp.
 template <class Pol, int MODE>
 __host__ __device__ constexpr size_t tile_region_bytes(int RN, int nwarps)
 {
     return (MODE == kModeFinal) ? 0 : (size_t)nwarps * RN * sizeof(typename Pol::Acc);
 }
+// The staging rounds share their space with the reduction of the indenter
+// force (2 kMaxBins bins and the total, doubles), which is done with before
+// the first round is staged.
+constexpr size_t kBinsBytes = (2 * kMaxBins + 2) * sizeof(double);
 template <class Pol, int MODE>
 __host__ __device__ constexpr size_t tile_dyn_bytes(int RN, int nwarps)
 {
-    return tile_region_bytes<Pol, MODE>(RN, nwarps) + (size_t)nwarps * 2 * sizeof(typename Pol::Stage);
+    return tile_region_bytes<Pol, MODE>(RN, nwarps) +
+           ((size_t)nwarps * Pol::kStages * sizeof(typename Pol::Stage) > kBinsBytes
+                ? (size_t)nwarps * Pol::kStages * sizeof(typename Pol::Stage)
+                : kBinsBytes);
 }
 
 // One substep of one tile (the body of k_tile_substep). Every return is
@@ -959,8 +976,6 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     extern __shared__ __align__(128) unsigned char s_dyn[];
     Acc *s_acc = reinterpret_cast<Acc *>(s_dyn);
     __shared__ uint64_t s_tma_bar;
-    __shared__ double s_bins[2 * kMaxBins];
-    __shared__ double s_tot[2];
     __shared__ int s_contact, s_mark[9];
     __shared__ typename Pol::Tables s_tab;
     // per lane of each of the warp's groups: its cell inside the tile
@@ -974,6 +989,9 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     const int GX = P.GridX, GY = P.GridY;
     const int p0 = R.tile_start[t], p1 = R.tile_start[t + 1];
     const int tid = threadIdx.x, nthr = blockDim.x;
+    // force bins and total of the tile's contact nodes, in the staging space
+    double *s_bins = reinterpret_cast<double *>(s_dyn + tile_region_bytes<Pol, MODE>(RN, nthr >> 5));
+    double *s_tot = s_bins + 2 * kMaxBins;
     Node *gA = (Node *)R.grid[R.bufA];
     Node *gB = (Node *)R.grid[R.bufB];
     const unsigned FULL = 0xffffffffu;
@@ -1141,6 +1159,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
             atomicAdd(&R.force_slot[0], s_tot[0]);
             atomicAdd(&R.force_slot[1], s_tot[1]);
         }
+        __syncthreads();  // the bins' space is staging space from here on
     }
     if (np == 0) return;
 
@@ -1153,16 +1172,20 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     // no longer its binned cell (it moved since binning) scatters on its
     // own: shared atomics inside the region, global atomics beyond it.
     const real h = Pol::h(P, K), m = Pol::mass(P, K), fhi = Pol::four_h_inv(P, K), sc = Pol::stress_c(P, K);
+    constexpr int kStages = Pol::kStages;
     int bad = 0;
     unsigned redo_count = 0, stray_count = 0, mlp_ok = 0, mlp_fb = 0;
     Acc *wacc = s_acc + warp * RN;
     typename Pol::Stage *stage =
-        reinterpret_cast<typename Pol::Stage *>(s_dyn + tile_region_bytes<Pol, MODE>(RN, nwarps)) + 2 * warp;
+        reinterpret_cast<typename Pol::Stage *>(s_dyn + tile_region_bytes<Pol, MODE>(RN, nwarps)) + kStages * warp;
 
-    // work items (k, r): round r of the warp's k-th group; the next item's
-    // particle state is copied into the other stage while this one computes
+    // work items (k, r): round r of the warp's k-th group (k = ng_w: none
+    // left); the particle state of the item kStages - 1 ahead is copied into
+    // its stage while this one computes
     auto next_item = [&](int k, int r, int &nk, int &nr) {
         nk = k;
+        nr = r;
+        if (k >= ng_w) return;
         nr = r + 1;
         if (nr >= s_wrounds[warp][k]) {
             nr = 0;
@@ -1171,18 +1194,25 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         }
     };
     auto issue = [&](int k, int r, int st) {
-        if (k < ng_w && r < (int)(s_wcnt[warp][k][lane] & 0xffffu)) Pol::prefetch(A, s_wgbase[warp][k] + 32 * r + lane, stage[st], lane);
+        if (k < ng_w && r < (int)(s_wcnt[warp][k][lane] & 0xffffu))
+            Pol::prefetch(A, s_wgbase[warp][k] + 32 * r + lane, stage[st], lane);
         __pipeline_commit();
     };
     int k = 0, r = 0, cur = 0;
     while (k < ng_w && s_wrounds[warp][k] == 0) k++;
+    // the items 1 .. kStages - 1 ahead of the current one
+    int qk[kStages - 1], qr[kStages - 1];
     issue(k, 0, 0);
+#pragma unroll
+    for (int a = 0; a < kStages - 1; a++) {
+        next_item(a == 0 ? k : qk[a - 1], a == 0 ? r : qr[a - 1], qk[a], qr[a]);
+        if (a < kStages - 2) issue(qk[a], qr[a], a + 1);
+    }
     CellSums<real> sums;
     while (k < ng_w) {
-        int nk, nr;
-        next_item(k, r, nk, nr);
-        issue(nk, nr, cur ^ 1);
-        __pipeline_wait_prior(1);
+        const int nk = qk[0], nr = qr[0];
+        issue(qk[kStages - 2], qr[kStages - 2], (cur + kStages - 1) % kStages);
+        __pipeline_wait_prior(kStages - 1);
         const uint32_t wc = s_wcnt[warp][k][lane];
         const int cl = (int)(wc >> 16);
         const int clx = cl % TX, cly = cl / TX;
@@ -1384,7 +1414,13 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         if (MODE != kModeFinal && nk != k) flush_cell_sums();
         k = nk;
         r = nr;
-        cur ^= 1;
+#pragma unroll
+        for (int a = 0; a < kStages - 2; a++) {
+            qk[a] = qk[a + 1];
+            qr[a] = qr[a + 1];
+        }
+        next_item(qk[kStages - 2], qr[kStages - 2], qk[kStages - 2], qr[kStages - 2]);
+        cur = cur + 1 == kStages ? 0 : cur + 1;
     }
     __pipeline_wait_prior(0);
     if (stray_count && R.strays) atomicAdd(R.strays, (unsigned long long)stray_count);
