@@ -34,7 +34,11 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-updates/s at 1M pts: FP32/learned vs plain FP64, 1 B200, ≤1% force err"
 UNIT = "particle-updates/s"
 L2_FLUSH_BYTES = 256 << 20
-SENS_NOISE = 3e-8  # std of the initial Fe perturbation of the FP64 sensitivity run
+# spread of the FP64 form itself: runs from an initial Fe perturbed by seeded
+# N(0, a^2) noise at each amplitude a, SPREAD_SEEDS seeds each
+SPREAD_AMPLITUDES, SPREAD_SEEDS = (1e-9, 1e-8, 3e-8), 5
+# workloads whose full 10,000-substep frame is compared with the CPU oracle
+ORACLE_WORKLOADS = ("c1_70k", "c2_250k")
 LATE_SUBSTEPS = 200  # launches timed after a full frame (crushed particles present)
 # learned projection: pairs harvested from the 250k-particle workload
 HARVEST_CONFIG, HARVEST_EVERY, HARVEST_CAP = "c2_250k", 5, 4_000_000
@@ -56,6 +60,8 @@ def parse():
     a.add_argument("--threads", type=int, default=128)
     a.add_argument("--no-e2e", action="store_true")
     a.add_argument("--no-accuracy", action="store_true")
+    a.add_argument("--no-oracle-accuracy", action="store_true",
+                   help="skip the full-frame comparisons with the CPU oracle (70k and 250k workloads)")
     a.add_argument("--no-cpu", action="store_true")
     a.add_argument("--no-fp64", action="store_true")
     a.add_argument("--no-surrogate", action="store_true")
@@ -188,10 +194,9 @@ def fused_min_bytes(form: str, n: int, na: int) -> float:
 def cpu_oracle_rate(name: str, budget_s: float, max_substeps: int, threads: int):
     """Particle-updates/s of the CPU FP64 oracle on the workload (a bounded
     sample: substeps until the time budget is spent)."""
-    from icempm_b200 import configs
     from oracle import oracle as orc
 
-    p, soa = configs.make_scene(name)
+    p, soa = orc.workload(name)
     grid = orc.new_grid(p)
     bins = np.zeros(2 * p.n_indenter_subdivisions)
     orc.run_substeps(p, soa, grid, bins, 1, threads=threads, history=False)  # warm
@@ -215,14 +220,16 @@ def host_threads():
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    from icempm_b200 import configs
     from oracle import oracle as orc
 
     threads = host_threads()
-    p, soa = configs.make_scene(args.config)
+    # parameters and particles from the oracle's own restatement of the
+    # workload set-up (bit-identical to the product's): this arm loads only
+    # oracle/libmpm_oracle.so
+    p, soa = orc.workload(args.config)
     grid = orc.new_grid(p)
     bins = np.zeros(2 * p.n_indenter_subdivisions)
-    sub = 2  # substeps per step: a bounded sample of the workload
+    sub = args.substeps  # substeps per step, as the GPU arm's step
     for _ in range(args.warmup):
         orc.run_substeps(p, soa, grid, bins, sub, threads=threads, history=False)
     times = []
@@ -345,7 +352,6 @@ def main():
     ms, (kms, klaunch) = timed(m, args.steps, args.warmup, args.substeps, ktime=True, clocks=clocks)
     total_s = rank_max(sum(ms) / 1e3)
     value = job_rate(world, n * args.substeps * args.steps, total_s)
-    redo = m.gpu.fp64_redo_count()
     m.gpu.close()
 
     hbm, peak_kind = peaks()
@@ -444,9 +450,12 @@ def main():
         for mm in pair:
             mm.gpu.close()
 
+        redo_frame = 0
         for form in (im.FORM_FP64, im.FORM_FP32, im.FORM_FP64_STEPWISE):
             mm = make(form, tile64 if form != im.FORM_FP32 else tile, threads64 if form != im.FORM_FP32 else None)
             mm.gpu.run_substeps(mm.prms, nsub)
+            if form == im.FORM_FP32:
+                redo_frame = mm.gpu.fp64_redo_count()
             if form != im.FORM_FP64_STEPWISE:
                 strays[form] = mm.gpu.stray_count()
             hist = mm.gpu.force_history(nsub)
@@ -459,19 +468,6 @@ def main():
         h64, s64, e64 = res[im.FORM_FP64]
         h32, s32, e32 = res[im.FORM_FP32]
         hsw, ssw, esw = res[im.FORM_FP64_STEPWISE]
-        # sensitivity of the FP64 form itself: the same run from an initial
-        # Fe perturbed by seeded N(0, 3e-8) noise
-        mm = make(im.FORM_FP64, tile64, threads64)
-        S = mm.gpu.soa()
-        S.Fe[:] += SENS_NOISE * np.random.default_rng(1).standard_normal(S.Fe.shape)
-        mm.gpu.transfer_ponts_to_device()
-        mm.gpu.run_substeps(mm.prms, nsub)
-        hps = mm.gpu.force_history(nsub)
-        mm.gpu.cuda_transfer_from_device()
-        mm.gpu.synchronize()
-        sps = mm.gpu.tmp_transfer_buffer.copy()
-        mm.gpu.close()
-        fps = np.hypot(hps[:, 0], hps[:, 1])
         f64 = np.hypot(h64[:, 0], h64[:, 1])
         f32 = np.hypot(h32[:, 0], h32[:, 1])
         fsw = np.hypot(hsw[:, 0], hsw[:, 1])
@@ -480,39 +476,82 @@ def main():
         def smooth(f):
             return f[: len(f) // win * win].reshape(-1, win).mean(axis=1)
         pitch = int(p0.nPtsPitch)
-        x64 = s64[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n]
-        x32 = s32[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n]
+
+        def pos(sbuf):
+            return sbuf[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n]
+        x64 = pos(s64)
+
+        def frame_errors(f, x):
+            """A frame's errors against the unperturbed FP64 fused frame."""
+            dx = np.abs(x - x64).max(axis=0) / p0.cellsize
+            return {"peak_force_rel_err": float(abs(f.max() - f64.max()) / max(f64.max(), 1e-30)),
+                    "peak_force_rel_err_100substep_avg": float(abs(smooth(f).max() - smooth(f64).max()) /
+                                                               max(smooth(f64).max(), 1e-30)),
+                    "frame_impulse_rel_err": float(abs(f.sum() - f64.sum()) / max(abs(f64.sum()), 1e-30)),
+                    "max_pos_err_h": float(dx.max()), "p99_pos_err_h": float(np.percentile(dx, 99))}
+
+        # spread of the FP64 form itself under tiny perturbations of the
+        # initial strain: the same frame from Fe + a N(0, 1) noise
+        spread = {}
+        for amp in SPREAD_AMPLITUDES:
+            runs = []
+            for seed in range(SPREAD_SEEDS):
+                mm = make(im.FORM_FP64, tile64, threads64)
+                S = mm.gpu.soa()
+                S.Fe[:] += amp * np.random.default_rng(1000 + seed).standard_normal(S.Fe.shape)
+                mm.gpu.transfer_ponts_to_device()
+                mm.gpu.run_substeps(mm.prms, nsub)
+                hp = mm.gpu.force_history(nsub)
+                mm.gpu.cuda_transfer_from_device()
+                mm.gpu.synchronize()
+                runs.append(frame_errors(np.hypot(hp[:, 0], hp[:, 1]), pos(mm.gpu.tmp_transfer_buffer)))
+                mm.gpu.close()
+            spread[f"{amp:g}"] = {k: sorted(r[k] for r in runs) for k in runs[0]}
+        e32f = frame_errors(f32, pos(s32))
+
+        def rank_in_spread(err):
+            """For each measure: the share of the perturbed FP64 runs (all
+            amplitudes) whose error is at least this one's."""
+            out = {}
+            for k, v in err.items():
+                allv = [x for a in spread.values() for x in a[k]]
+                out[k] = float(np.mean([x >= v for x in allv])) if allv else None
+            return out
+
         extra["accuracy"] = {
-            "substeps": nsub, "against": "fp64 fused form on the GPU (parity-tested against the CPU FP64 oracle)",
+            "substeps": nsub,
+            "against": "fp64 fused form on the GPU, which tracks the CPU FP64 oracle to ~1e-12 over 10,000 "
+                       "substeps on the 70k and 250k workloads (oracle section) and over 200 substeps here",
             "fp32_state_err_after_substeps": early,
             "peak_force_fp64_N": float(f64.max()), "peak_force_fp32_N": float(f32.max()),
-            "peak_force_rel_err": float(abs(f32.max() - f64.max()) / max(f64.max(), 1e-30)),
+            "fp32": e32f,
+            "fp32_share_of_fp64_spread_at_least_as_large": rank_in_spread(e32f),
             "force_history_rel_l2": float(np.linalg.norm(f32 - f64) / max(np.linalg.norm(f64), 1e-30)),
-            "max_pos_err_h": float(np.abs(x32 - x64).max() / p0.cellsize),
-            "p99_pos_err_h": float(np.percentile(np.abs(x32 - x64).max(axis=0), 99) / p0.cellsize),
-            "peak_force_rel_err_100substep_avg": float(abs(smooth(f32).max() - smooth(f64).max()) /
-                                                       max(smooth(f64).max(), 1e-30)),
-            "frame_impulse_rel_err": float(abs(f32.sum() - f64.sum()) / max(abs(f64.sum()), 1e-30)),
-            "fp64_vs_fp64_stepwise": {
-                "peak_force_rel_err": float(abs(fsw.max() - f64.max()) / max(f64.max(), 1e-30)),
-                "peak_force_rel_err_100substep_avg": float(abs(smooth(fsw).max() - smooth(f64).max()) /
-                                                           max(smooth(f64).max(), 1e-30)),
-                "max_pos_err_h": float(np.abs(ssw[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n] - x64).max() /
-                                       p0.cellsize),
-            },
-            "fp64_perturbed_vs_fp64": {
-                "initial_fe_noise": SENS_NOISE,
-                "peak_force_rel_err": float(abs(fps.max() - f64.max()) / max(f64.max(), 1e-30)),
-                "max_pos_err_h": float(np.abs(sps[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n] - x64).max() /
-                                       p0.cellsize),
-                "p99_pos_err_h": float(np.percentile(np.abs(sps[4 * pitch: 6 * pitch].reshape(2, pitch)[:, :n] -
-                                                            x64).max(axis=0), 99) / p0.cellsize),
-            },
+            "fp64_spread_under_initial_strain_noise": {
+                "seeds": SPREAD_SEEDS, "errors_sorted_by_amplitude": spread,
+                "what": "FP64 fused frames from Fe + a N(0,1) (seeded), against the unperturbed FP64 frame"},
+            "fp64_vs_fp64_stepwise": frame_errors(fsw, pos(ssw)),
             "error_flags": [int(e64), int(e32), int(esw)],
             "late_frame_us_per_launch": late,
-            "fp64_fallback_particles": redo,
+            "fp64_redo_per_substep": redo_frame / nsub,
             "stray_particle_substeps": {"fp64": strays.get(im.FORM_FP64), "fp32": strays.get(im.FORM_FP32)},
         }
+        # full frames of the smaller workloads against the CPU FP64 oracle
+        if not args.no_oracle_accuracy:
+            from tests.tracking import track
+
+            vs = {}
+            for cname in ORACLE_WORKLOADS:
+                pc, soac = configs.make_scene(cname)
+                ns_c = configs.CONFIGS[cname][6]
+                cps = (1, 10, 100, 1000, ns_c)
+                t0 = time.perf_counter()
+                r = track(pc, soac, (im.FORM_FP64_STEPWISE, im.FORM_FP64, im.FORM_FP32), cps, host_threads())
+                r["particles"] = int(pc.nPts)
+                r["substeps"] = ns_c
+                r["seconds"] = time.perf_counter() - t0
+                vs[cname] = r
+            extra["accuracy"]["vs_cpu_oracle"] = vs
 
         # --- the learned projection: pairs harvested from the FP32 form on the
         # 250k-particle workload, trained on the tensor cores, then the
@@ -583,14 +622,8 @@ def main():
                              "final_loss": float(loss[-100:].mean()), "harvest_s": t1 - t0, "train_s": t2 - t1},
                 "tolerance": SUR_TOL,
                 "network_projections_accepted": acc_n, "exact_projections": exact_n,
-                "accuracy_vs_fp64": {
-                    "peak_force_rel_err": float(abs(fs.max() - f64.max()) / max(f64.max(), 1e-30)),
-                    "peak_force_rel_err_100substep_avg": float(abs(smooth(fs).max() - smooth(f64).max()) /
-                                                               max(smooth(f64).max(), 1e-30)),
-                    "frame_impulse_rel_err": float(abs(fs.sum() - f64.sum()) / max(abs(f64.sum()), 1e-30)),
-                    "max_pos_err_h": float(np.abs(xs - x64).max() / p0.cellsize),
-                    "p99_pos_err_h": float(np.percentile(np.abs(xs - x64).max(axis=0), 99) / p0.cellsize),
-                },
+                "accuracy_vs_fp64": frame_errors(fs, xs),
+                "share_of_fp64_spread_at_least_as_large": rank_in_spread(frame_errors(fs, xs)),
             }
 
     # --- the 64-case ensemble: every case as its own run_substeps (one after

@@ -82,7 +82,7 @@ def build_oracle(force: bool = False) -> None:
     reference's own SVD and substep code for the host (oracle/_ref; test
     infrastructure)."""
     target = os.path.join(ORACLE, "libmpm_oracle.so")
-    if force or _stale(target, [os.path.join(ORACLE, "mpm_oracle.c"),
+    if force or _stale(target, [os.path.join(ORACLE, "mpm_oracle.c"), os.path.join(ORACLE, "scene_oracle.c"),
                                 os.path.join(ROOT, "include", "icempm_params.h")]):
         _run(["make", "-C", ORACLE, "libmpm_oracle.so"] + (["-B"] if force else []))
     refs = [os.path.join(ORACLE, "_ref", f) for f in ("libref_svd.so", "libref_step.so")]

@@ -7,6 +7,7 @@ never imports it.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -41,6 +42,7 @@ def lib():
             "oracle_compute_pq": (None, [P, vp, vp]),
             "oracle_grain_params": (None, [P, C.c_short, vp]),
             "oracle_failure_check": (i, [P, C.c_short, d, d]),
+            "oracle_scene_block": (C.c_long, [P, i, i, d, d, C.c_uint64, vp]),
         }
         for n, (r, a) in sigs.items():
             f = getattr(L, n)
@@ -105,6 +107,97 @@ def grain_params(prms, grain):
 
 def failure_check(prms, grain, p, q) -> int:
     return int(lib().oracle_failure_check(C.byref(prms), int(grain), float(p), float(q)))
+
+
+# ----------------------------------------------------------- parameters
+# icy::SimParams set-up restated (simulation/parameters_sim.cpp): Reset
+# (:5-56), the numeric keys of ParseFile (:73-98) and the derived constants
+# (:121-147), in the reference's operation order, so that the CPU arm of
+# bench.py builds its parameter block without the product library.
+
+_DOUBLE_KEYS = ("InitialTimeStep", "YoungsModulus", "GridXDimension", "ParticleViewSize", "SimulationEndTime",
+                "PoissonsRatio", "Gravity", "Density", "IndDiameter", "IndVelocity", "IndDepth",
+                "IceCompressiveStrength", "IceTensileStrength", "IceShearStrength", "DP_threshold_p",
+                "GrainVariability")
+_INT_KEYS = ("GridX", "GridY", "UseWarpLevelReduction", "tpb_P2G", "tpb_Upd", "tpb_G2P", "SortPointsByGridCell")
+
+
+def _derive(p):
+    """ComputeCamClayParams2 (with ComputeLame) and ComputeHelperVariables."""
+    E, nu = p.YoungsModulus, p.PoissonsRatio
+    p.lambda_ = E * nu / ((1 + nu) * (1 - 2 * nu))
+    p.mu = E / (2 * (1 + nu))
+    p.kappa = p.mu * 2. / 3. + p.lambda_
+    p.NACC_beta = p.IceTensileStrength / p.IceCompressiveStrength
+    beta, q, p0 = p.NACC_beta, p.IceShearStrength, p.IceCompressiveStrength
+    p.NACC_M = (2 * q * math.sqrt(1 + 2 * beta)) / (p0 * (1 + beta))
+    p.NACC_Msq = p.NACC_M * p.NACC_M
+    p.UpdateEveryNthStep = int(1.0 / (200 * p.InitialTimeStep))
+    p.cellsize = p.GridXDimension / p.GridX
+    p.cellsize_inv = 1. / p.cellsize
+    p.Dp_inv = 4. / (p.cellsize * p.cellsize)
+    p.IndRSq = p.IndDiameter * p.IndDiameter / 4.
+    p.GridTotal = p.GridX * p.GridY
+
+
+def params(values: dict):
+    """A parameter block: Reset, then the configuration values (as ParseFile
+    reads them; DP_phi in degrees), then the derived constants."""
+    from icempm_b200 import SimParams  # the ctypes layout only
+
+    p = SimParams()
+    C.memset(C.byref(p), 0, C.sizeof(p))
+    pi = 3.14159265358979323846
+    p.n_indenter_subdivisions = 100
+    p.InitialTimeStep = 3.e-5
+    p.YoungsModulus = 5.e8
+    p.GridX, p.GridY = 128, 55
+    p.ParticleViewSize = 2.5
+    p.GridXDimension = 3.33
+    p.SimulationEndTime = 12
+    p.PoissonsRatio, p.Gravity, p.Density = 0.3, 9.81, 980
+    p.IndDiameter, p.IndVelocity, p.IndDepth = 0.324, 0.2, 0.25
+    p.IceCompressiveStrength, p.IceTensileStrength, p.IceShearStrength = 100e6, 1e6, 0.5e6
+    p.DP_tan_phi = math.tan(30 * pi / 180.)
+    p.DP_threshold_p = 1e3
+    p.tpb_P2G, p.tpb_Upd, p.tpb_G2P = 256, 512, 128
+    p.GrainVariability = 0.50
+    p.SortPointsByGridCell = 1
+    _derive(p)
+    for k in _DOUBLE_KEYS:
+        if k in values:
+            setattr(p, k, float(values[k]))
+    for k in _INT_KEYS:
+        if k in values:
+            setattr(p, k, int(values[k]))
+    if "DP_phi" in values:
+        p.DP_tan_phi = math.tan(float(values["DP_phi"]) * pi / 180)
+    _derive(p)
+    return p
+
+
+def scene_block(p, cells_x: int, cells_y: int, ind_y_above_floor: float, grain_size: float, seed: int):
+    """The seeded synthetic block (oracle/scene_oracle.c); fills p and
+    returns the particle SoA (16 rows of the 64-aligned pitch)."""
+    n = 4 * cells_x * cells_y
+    pitch = (n + 63) // 64 * 64
+    soa = np.zeros(16 * pitch, dtype=np.float64)
+    got = lib().oracle_scene_block(C.byref(p), cells_x, cells_y, ind_y_above_floor, grain_size, seed, _p(soa))
+    if got != n:
+        raise RuntimeError("oracle_scene_block failed")
+    p.nPtsPitch = pitch
+    p.nGridPitch = (p.GridTotal + 63) // 64 * 64
+    return soa
+
+
+def workload(name: str, seed: int = 12345):
+    """(params, SoA) of a benchmark workload (icempm_b200.configs.CONFIGS),
+    built by the oracle alone."""
+    from icempm_b200 import configs  # the workload table (data only)
+
+    gx, gy, dim, dt, cx, cy, _ = configs.CONFIGS[name]
+    p = params(dict(configs.MATERIAL, GridX=gx, GridY=gy, GridXDimension=dim, InitialTimeStep=dt))
+    return p, scene_block(p, cx, cy, 0.2, 0.05, seed)
 
 
 def _p(a: np.ndarray):

@@ -8,7 +8,7 @@ import icempm_b200 as im
 from icempm_b200 import configs
 from icempm_b200.ensemble import Ensemble
 
-from mpm_cases import compare_states, gpu_model, gpu_state, params, scene
+from mpm_cases import compare_states, gpu_model, gpu_state, oracle_run, params, scene
 
 CASES = [  # (cells, seed, overrides)
     ((40, 10), 3, dict(YoungsModulus=8e8, IndVelocity=0.5)),
@@ -300,6 +300,49 @@ def test_ensemble_surrogate_form_matches_cases_run_alone():
         assert err["disp_h"] <= 1e-3, err
         assert np.percentile(per, 99) <= 2e-2, np.percentile(per, 99)
         assert m.gpu.error_code == 0
+    ens.close()
+    for m in models:
+        m.gpu.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,tol_pos,tol", [(im.FORM_FP64, 1e-9, 1e-9), (im.FORM_FP32, 1e-4, 1e-3)])
+def test_ensemble_cases_match_the_oracle(form, tol_pos, tol):
+    """Cases of different sizes, grids, materials and indenters in one
+    ensemble, each compared with the CPU FP64 oracle directly, over 13
+    substeps that cross three re-binnings (every 4 substeps). The states
+    carry crushed particles, Jp_inv != 1 and sheared Fe, so every branch of
+    the constitutive model runs. Tolerances: FP64 1e-9 (reordered float
+    atomics); FP32 1e-4 h in position and 1e-3 of the velocity and strain
+    scales."""
+    n, rebin = 13, 4
+    specs = [((96, 48), 0.75, (40, 10), 3, dict(YoungsModulus=8e8, IndVelocity=0.5)),
+             ((64, 32), 0.5, (24, 8), 5, dict(YoungsModulus=2e9, IndVelocity=1.0, DP_phi=50)),
+             ((128, 40), 1.0, (56, 8), 9, dict(IndVelocity=0.2, IndDiameter=0.2))]
+    cases = []
+    for grid, dim, cells, seed, over in specs:
+        p = params(*grid, dim=dim, **over)
+        cases.append((p, scene(p, cells=cells, seed=seed, ind_y=0.03, vel=0.05, perturb=5e-4, crushed_frac=0.2,
+                               jp_spread=0.005)))
+    ens = Ensemble(form, tile=1, threads=128)
+    ens.set(rebin_interval=rebin)
+    models = []
+    for p, soa in cases:
+        m = gpu_model(p, soa, form, tile=1, threads=128)
+        ens.add(m)
+        models.append(m)
+    ens.run(n)
+    for (p, soa), m in zip(cases, models):
+        got, hist = gpu_state(m), m.gpu.force_history(n)
+        q, ref, _, oerr, href = oracle_run(p, soa, n, threads=4)
+        assert oerr == 0 and m.gpu.error_code == 0
+        assert m.prms.SimulationStep == q.SimulationStep and m.prms.indenter_x == q.indenter_x
+        err = compare_states(p, got, ref, soa)
+        assert err["disp_h"] <= tol_pos and err["strain"] <= tol and err["vel"] <= tol, err
+        assert err["crushed_mismatch"] <= (0 if form == im.FORM_FP64 else max(2, p.nPts // 1000)), err
+        assert err["grain_mismatch"] == 0
+        scale = max(np.abs(href).max(), 1e-30)
+        assert np.abs(hist - href).max() <= (1e-9 if form == im.FORM_FP64 else 1e-3) * scale
     ens.close()
     for m in models:
         m.gpu.close()
