@@ -758,16 +758,8 @@ static int tile_order(icm_ctx *c, int ntiles, const int *&order, int &nlaunch)
         return ICM_OK;
     }
     if (ntiles > kMaxOrderTiles) return ICM_OK;
-    int m = 1;
-    while (m < ntiles) m <<= 1;
-    static bool opted = false;
-    if (!opted) {
-        ICM_CUDA(cudaFuncSetAttribute(k_tile_order, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(sizeof(unsigned long long) * kMaxOrderTiles)));
-        opted = true;
-    }
     const int max_split = std::min(std::max(c->split_max, 0), ntiles);
-    k_tile_order<<<1, kOrderThreads, sizeof(unsigned long long) * m, c->stream>>>(
+    k_tile_order<<<1, kOrderThreads, sizeof(int) * (size_t)ntiles, c->stream>>>(
         ntiles, c->fz.cost, c->bin.tile_start, max_split, (float)c->split_ratio, c->fz.order);
     ICM_LAUNCHED("k_tile_order");
     c->pdl_next = false;  // the substep reads the order before its dependency wait

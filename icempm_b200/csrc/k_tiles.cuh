@@ -1597,80 +1597,8 @@ template <class Pol> __global__ void k_ens_check(const EnsCase<Pol> *__restrict_
     if (__syncthreads_or(lost) && threadIdx.x == 0) atomicOr(c.R.err, 2);
 }
 
-// Tile order by descending cost (ties by tile index): a bitonic sort of
-// (cost << 32 | ~tile) keys in shared memory, one CTA, n <= kMaxOrderTiles.
-// A tile's cost is cost[t] + cost[n + t] (its halves when it ran split).
-// The heaviest tiles whose cost exceeds ratio times the mean over tiles
-// holding particles, at most max_split of them, are split: their two halves
-// lead the order (two CTAs each), then the other tiles; the order has
-// n + max_split entries, the unused ones -1.
 constexpr int kMaxOrderTiles = 8192;
 constexpr int kOrderThreads = 1024;
-
-__global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsigned *cost, const int *tile_start,
-                                                              int max_split, float ratio, int *order)
-{
-    extern __shared__ unsigned long long s_key[];
-    __shared__ unsigned long long s_sum;
-    __shared__ int s_busy, s_nsplit;
-    int m = 1;
-    while (m < n) m <<= 1;
-    if (threadIdx.x == 0) {
-        s_sum = 0;
-        s_busy = 0;
-        s_nsplit = 0;
-    }
-    __syncthreads();
-    unsigned long long sum = 0;
-    int busy = 0;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        unsigned c = 0;
-        // a tile without particles (its cost may still be the one measured
-        // before a re-binning emptied it) sorts last and is never split
-        if (i < n && tile_start[i + 1] > tile_start[i]) {
-            const unsigned long long cc = (unsigned long long)cost[i] + cost[n + i];
-            c = cc > 0xffffffffull ? 0xffffffffu : (unsigned)cc;
-            sum += c;
-            busy++;
-        }
-        s_key[i] = (i < n) ? (((unsigned long long)c << 32) | (0xffffffffu - (unsigned)i)) : 0ull;
-    }
-    atomicAdd(&s_sum, sum);
-    atomicAdd(&s_busy, busy);
-    __syncthreads();
-    for (int k = 2; k <= m; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < m; i += blockDim.x) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const unsigned long long a = s_key[i], b = s_key[l];
-                    const bool desc = (i & k) == 0;
-                    if (desc ? (a < b) : (a > b)) {
-                        s_key[i] = b;
-                        s_key[l] = a;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    // the split tiles are a prefix of the sorted list
-    const double thr = s_busy > 0 ? (double)ratio * (double)s_sum / (double)s_busy : 1e300;
-    const int lim = min(max_split, n);
-    for (int i = threadIdx.x; i < lim; i += blockDim.x)
-        if ((double)(s_key[i] >> 32) > thr && (i + 1 == lim || (double)(s_key[i + 1] >> 32) <= thr))
-            s_nsplit = i + 1;
-    __syncthreads();
-    const int S = s_nsplit;
-    for (int i = threadIdx.x; i < n + max_split; i += blockDim.x) {
-        int v = -1;
-        if (i < 2 * S) {
-            v = (int)(0xffffffffu - (unsigned)(s_key[i >> 1] & 0xffffffffu)) | kSplitBit | ((i & 1) ? kHalfBit : 0);
-        } else if (i < n + S) {
-            v = (int)(0xffffffffu - (unsigned)(s_key[i - S] & 0xffffffffu));
-        }
-        order[i] = v;
-    }
-}
 
 // ------------------------------------------------ binning, pack and unpack
 
@@ -1727,6 +1655,96 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *tmp, int &total)
     total = tmp[(blockDim.x >> 5) - 1];
     __syncthreads();
     return before;
+}
+
+// Tile order by descending cost (one CTA, n <= kMaxOrderTiles): a
+// counting sort on the cost quantised to kOrderLevels levels of the
+// largest cost. Inside a level the order is the order in which threads
+// claim places; nothing depends on it, since a substep's result does not
+// depend on the order its CTAs run in. A tile's cost is
+// cost[t] + cost[n + t] (its halves when it ran split); a tile without
+// particles (whose cost may be one measured before a re-binning emptied
+// it) counts as 0 and sorts last. The first S tiles of the order are split,
+// S = the number of tiles whose cost exceeds ratio times the mean over
+// tiles holding particles, at most max_split: their two halves lead the
+// order (two CTAs each), then the other tiles; the order has n + max_split
+// entries, the unused ones -1. Dynamic shared memory: n ints.
+constexpr int kOrderLevels = kOrderThreads;
+
+__global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsigned *cost, const int *tile_start,
+                                                              int max_split, float ratio, int *order)
+{
+    extern __shared__ int s_sorted[];
+    __shared__ int s_off[kOrderLevels];
+    __shared__ int s_tmp[32];
+    __shared__ unsigned long long s_sum;
+    __shared__ unsigned s_max;
+    __shared__ int s_busy, s_over;
+    const int tid = threadIdx.x;
+    for (int b = tid; b < kOrderLevels; b += blockDim.x) s_off[b] = 0;
+    if (tid == 0) {
+        s_sum = 0;
+        s_max = 0;
+        s_busy = 0;
+        s_over = 0;
+    }
+    __syncthreads();
+    auto tile_cost = [&](int i) -> unsigned {
+        if (tile_start[i + 1] <= tile_start[i]) return 0u;
+        const unsigned long long cc = (unsigned long long)cost[i] + cost[n + i];
+        return cc > 0xffffffffull ? 0xffffffffu : (unsigned)cc;
+    };
+    unsigned long long sum = 0;
+    unsigned mx = 0;
+    int busy = 0;
+    for (int i = tid; i < n; i += blockDim.x) {
+        const unsigned c = tile_cost(i);
+        if (tile_start[i + 1] > tile_start[i]) {
+            sum += c;
+            busy++;
+        }
+        mx = max(mx, c);
+    }
+    atomicAdd(&s_sum, sum);
+    atomicAdd(&s_busy, busy);
+    atomicMax(&s_max, mx);
+    __syncthreads();
+    const unsigned cmax = s_max;
+    // level kOrderLevels - 1 holds the heaviest tiles, level 0 the empty ones
+    auto level = [&](unsigned c) -> int {
+        return c == 0u ? 0 : 1 + (int)((unsigned long long)c * (kOrderLevels - 2) / cmax);
+    };
+    const double thr = s_busy > 0 ? (double)ratio * (double)s_sum / (double)s_busy : 1e300;
+    int over = 0;
+    for (int i = tid; i < n; i += blockDim.x) {
+        const unsigned c = tile_cost(i);
+        atomicAdd(&s_off[level(c)], 1);
+        over += (double)c > thr;
+    }
+    atomicAdd(&s_over, over);
+    __syncthreads();
+    // start of each level in descending level order: thread t takes level
+    // kOrderLevels - 1 - t (blockDim.x == kOrderLevels)
+    {
+        const int b = kOrderLevels - 1 - tid;
+        int total;
+        const int before = block_exclusive_scan(s_off[b], s_tmp, total);
+        __syncthreads();
+        s_off[b] = before;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) s_sorted[atomicAdd(&s_off[level(tile_cost(i))], 1)] = i;
+    __syncthreads();
+    const int S = min(min(s_over, max_split), n);
+    for (int i = tid; i < n + max_split; i += blockDim.x) {
+        int v = -1;
+        if (i < 2 * S) {
+            v = s_sorted[i >> 1] | kSplitBit | ((i & 1) ? kHalfBit : 0);
+        } else if (i < n + S) {
+            v = s_sorted[i - S];
+        }
+        order[i] = v;
+    }
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_chunks(const int *in, int n, int *chunk_sums)
@@ -1817,6 +1835,14 @@ __global__ void __launch_bounds__(256) k_lane_order(int cells_per_tile, const in
 {
     __shared__ uint32_t s_key[kMaxTileCells];
     const int base = blockIdx.x * cells_per_tile, n = cells_per_tile;
+    if (cell_start[base + n] == cell_start[base]) {
+        // no particles: every count is 0, and the order by key is the identity
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            lane_cell[base + i] = base + i;
+            cell_lane[base + i] = base + i;
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int cnt = min(cell_start[base + i + 1] - cell_start[base + i], 0xffff);
         s_key[i] = ((uint32_t)(0xffff - cnt) << 16) | (uint32_t)i;  // ascending key = descending count

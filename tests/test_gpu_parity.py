@@ -257,3 +257,46 @@ def test_rebinning_keeps_parity(form):
     else:
         assert e["disp_h"] < 1e-4 and e["vel"] < 5e-3, e
     assert e["grain_mismatch"] == 0
+
+
+@pytest.mark.parametrize("form", [im.FORM_FP64, im.FORM_FP32])
+def test_emptied_tile_next_to_the_indenter_is_not_split(form):
+    """A strip of particles starts in the second column of 16x8 tiles and
+    moves left at 400 m/s into the first, so the tile it leaves keeps a
+    measured cost while it holds no particles (from substep 20 on). Its
+    first node columns still get mass from the strip's stencils, and the
+    indenter touches them. With
+    every measured tile split (ratio 0) and a re-binning every 2 substeps,
+    the emptied tile must run whole: its reaction force counts once, and the
+    force history matches the oracle."""
+    p = params(96, 48, dim=0.75, dt=2e-6, IndDiameter=0.02)
+    soa = scene(p, cells=(2, 6), seed=31, ind_y=0.03)
+    S = im.SoA(soa, p.nPtsPitch, p.nPts)
+    h = p.cellsize
+    S.pos[0] += 16.6 * h - S.pos[0].min()      # bases 16 and 17: the second tile column
+    S.pos[1] += 8.3 * h - S.pos[1].min()       # tile row 1 (y cells 8..13; stencils reach node row 15)
+    S.vel[0] = -400.0
+    S.vel[1] = 0.0
+    S.Bp[:] = 0.0
+    # above the strip: it touches node row 15 of the emptied tile without stopping the strip
+    p.indenter_x = p.indenter_x_initial = 16.5 * h
+    p.indenter_y = p.indenter_y_initial = 15.6 * h
+    n = 30
+    m = gpu_model(p, soa, form, 0, 128)
+    m.gpu.set_rebin_interval(2)
+    m.gpu.set_tile_split(4096, 0.0)
+    m.gpu.run_substeps(m.prms, n)
+    got = gpu_state(m)
+    fh = m.gpu.force_history(n)
+    q, ref, bins, err, hist = oracle_run(p, soa, n)
+    R = im.SoA(ref, p.nPtsPitch, p.nPts)
+    assert (R.pos[0] / h - 0.5).astype(int).max() <= 15   # the strip has left the second tile
+    assert np.abs(hist[-10:]).max() > 0                   # and the indenter still pushes it
+    e = compare_states(p, got, ref, soa)
+    if form == im.FORM_FP64:
+        assert max(e["disp_rel"], e["vel"], e["strain"]) < FP64_TOL, e
+        assert max_rel(fh, hist) < FP64_TOL
+    else:
+        assert e["disp_h"] < 1e-4 and e["vel"] < 5e-3, e
+        assert max_rel(fh, hist) < 1e-2
+    assert m.gpu.error_code == 0
