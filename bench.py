@@ -183,11 +183,12 @@ def alg_bytes(form: str, n: int, na: int, ng: int) -> float:
 
 def fused_min_bytes(form: str, n: int, na: int) -> float:
     """Bytes the fused one-launch substep must move at least (its own data
-    layout): fp32 particle state read 36 B (cell 4, fraction 8, H 16, Jp 4,
-    meta 4) + written 28 B, grid 48 B per active node (read 16, scatter 16,
-    zero 16); fp64 read 60 B + written 48 B, grid 96 B per active node."""
+    layout): fp32 particle state read 36 B (fraction, cell and meta word in
+    one 16-byte vector, H 16, Jp 4) + written 32 B, grid 48 B per active node
+    (read 16, scatter 16, zero 16); fp64 read 60 B + written 48 B, grid 96 B
+    per active node."""
     if form == "fp32":
-        return 64.0 * n + 48.0 * na
+        return 68.0 * n + 48.0 * na
     return 108.0 * n + 96.0 * na
 
 

@@ -247,8 +247,8 @@ static void free_spare(icm_ctx *c)
 {
     dfree(c->fz.s64.pos); dfree(c->fz.s64.F); dfree(c->fz.s64.Jp); dfree(c->fz.s64.meta);
     dfree(c->fz.s64.vel); dfree(c->fz.s64.Bp); dfree(c->fz.s64.pq);
-    dfree(c->fz.s32.cell); dfree(c->fz.s32.frac); dfree(c->fz.s32.H); dfree(c->fz.s32.Jp);
-    dfree(c->fz.s32.meta); dfree(c->fz.s32.vel); dfree(c->fz.s32.Bp); dfree(c->fz.s32.pq);
+    dfree(c->fz.s32.X); dfree(c->fz.s32.H); dfree(c->fz.s32.Jp);
+    dfree(c->fz.s32.vel); dfree(c->fz.s32.Bp); dfree(c->fz.s32.pq);
     dfree(c->fz.spare_pid);
     dfree(c->fz.slot_key);
     c->fz.spare_cap = 0;
@@ -259,8 +259,8 @@ static void free_fused(icm_ctx *c)
     free_spare(c);
     dfree(c->fz.p64.pos); dfree(c->fz.p64.F); dfree(c->fz.p64.Jp); dfree(c->fz.p64.meta);
     dfree(c->fz.p64.vel); dfree(c->fz.p64.Bp); dfree(c->fz.p64.pq);
-    dfree(c->fz.p32.cell); dfree(c->fz.p32.frac); dfree(c->fz.p32.H); dfree(c->fz.p32.Jp);
-    dfree(c->fz.p32.meta); dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
+    dfree(c->fz.p32.X); dfree(c->fz.p32.H); dfree(c->fz.p32.Jp);
+    dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
     for (int b = 0; b < 3; b++) { if (c->fz.grid[b]) cudaFree(c->fz.grid[b]); c->fz.grid[b] = nullptr; }
     dfree(c->fz.dirty);
     dfree(c->fz.cost); dfree(c->fz.order);
@@ -344,8 +344,8 @@ static int ensure_slots(icm_ctx *c, int form, size_t nslots)
     if (c->fz.form == form && c->fz.cap_pts >= nslots && c->bin.cap_slots >= nslots) return ICM_OK;
     dfree(c->fz.p64.pos); dfree(c->fz.p64.F); dfree(c->fz.p64.Jp); dfree(c->fz.p64.meta);
     dfree(c->fz.p64.vel); dfree(c->fz.p64.Bp); dfree(c->fz.p64.pq);
-    dfree(c->fz.p32.cell); dfree(c->fz.p32.frac); dfree(c->fz.p32.H); dfree(c->fz.p32.Jp);
-    dfree(c->fz.p32.meta); dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
+    dfree(c->fz.p32.X); dfree(c->fz.p32.H); dfree(c->fz.p32.Jp);
+    dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
     dfree(c->bin.pid);
     free_spare(c);
     // the same headroom as the spare set: re-binning swaps the two sets, and
@@ -364,8 +364,8 @@ static int ensure_slots(icm_ctx *c, int form, size_t nslots)
             return rc;
     } else {
         Parts32 &A = c->fz.p32;
-        if ((rc = dalloc(&A.cell, nslots)) || (rc = dalloc(&A.frac, nslots)) || (rc = dalloc(&A.H, nslots)) ||
-            (rc = dalloc(&A.Jp, nslots)) || (rc = dalloc(&A.meta, nslots)) || (rc = dalloc(&A.vel, nslots)) ||
+        if ((rc = dalloc(&A.X, nslots)) || (rc = dalloc(&A.H, nslots)) ||
+            (rc = dalloc(&A.Jp, nslots)) || (rc = dalloc(&A.vel, nslots)) ||
             (rc = dalloc(&A.Bp, nslots)) || (rc = dalloc(&A.pq, nslots)))
             return rc;
     }
@@ -564,8 +564,8 @@ static int ensure_spare(icm_ctx *c, size_t nslots)
             return rc;
     } else {
         Parts32 &A = c->fz.s32;
-        if ((rc = dalloc(&A.cell, nslots)) || (rc = dalloc(&A.frac, nslots)) || (rc = dalloc(&A.H, nslots)) ||
-            (rc = dalloc(&A.Jp, nslots)) || (rc = dalloc(&A.meta, nslots)) || (rc = dalloc(&A.vel, nslots)) ||
+        if ((rc = dalloc(&A.X, nslots)) || (rc = dalloc(&A.H, nslots)) ||
+            (rc = dalloc(&A.Jp, nslots)) || (rc = dalloc(&A.vel, nslots)) ||
             (rc = dalloc(&A.Bp, nslots)) || (rc = dalloc(&A.pq, nslots)))
             return rc;
     }

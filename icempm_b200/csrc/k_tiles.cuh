@@ -248,11 +248,18 @@ __device__ __forceinline__ bool tma_region_wait(uint64_t *bar, int *err)
 }
 
 struct Parts64 { double2 *pos; double4 *F; double *Jp; uint32_t *meta; double2 *vel; double4 *Bp; double2 *pq; };
-struct Parts32 { uint32_t *cell; float2 *frac; float4 *H; float *Jp; uint32_t *meta; float2 *vel; float4 *Bp; float2 *pq; };
+// FP32 form: X = {fraction x, fraction y, cell (pack_cell bits), meta word
+// (bits)}, one 16-byte vector, so that a particle's position and flags move
+// in one copy; H = Fe - I.
+struct Parts32 { float4 *X; float4 *H; float *Jp; float2 *vel; float4 *Bp; float2 *pq; };
 
 __host__ __device__ __forceinline__ uint32_t pack_cell(int ix, int iy) { return (uint32_t)(uint16_t)(int16_t)ix | ((uint32_t)(uint16_t)(int16_t)iy << 16); }
 __device__ __forceinline__ int cell_x(uint32_t c) { return (int)(int16_t)(uint16_t)(c & 0xffffu); }
 __device__ __forceinline__ int cell_y(uint32_t c) { return (int)(int16_t)(uint16_t)(c >> 16); }
+__device__ __forceinline__ float4 pack_x32(int ix, int iy, float fx, float fy, uint32_t meta)
+{
+    return make_float4(fx, fy, __uint_as_float(pack_cell(ix, iy)), __uint_as_float(meta));
+}
 
 // Symmetric Kirchhoff stress as the P2G needs it.
 template <class T> struct Tau { T t00, t01, t10, t11; };
@@ -415,28 +422,28 @@ struct Pol32 {
     struct St { int ix, iy; float fx, fy; M2f H; float Jp; uint32_t meta; };
     struct Sten { int bx, by; float fx, fy, wx[3], wy[3]; };
     // one round of a warp (32 particles) staged in shared memory
-    struct Stage { float4 H[32]; float2 frac[32]; uint32_t cell[32]; float Jp[32]; uint32_t meta[32]; };
+    struct Stage { float4 H[32]; float4 X[32]; float Jp[32]; };
 
     static __device__ __forceinline__ void prefetch(const Parts &A, int p, Stage &S, int lane)
     {
         __pipeline_memcpy_async(&S.H[lane], &A.H[p], 16);
-        __pipeline_memcpy_async(&S.frac[lane], &A.frac[p], 8);
-        __pipeline_memcpy_async(&S.cell[lane], &A.cell[p], 4);
+        __pipeline_memcpy_async(&S.X[lane], &A.X[p], 16);
         __pipeline_memcpy_async(&S.Jp[lane], &A.Jp[p], 4);
-        __pipeline_memcpy_async(&S.meta[lane], &A.meta[p], 4);
+    }
+    static __device__ __forceinline__ St unpack(const float4 X, const float4 H, float Jp)
+    {
+        St s;
+        const uint32_t c = __float_as_uint(X.z);
+        s.ix = cell_x(c); s.iy = cell_y(c);
+        s.fx = X.x; s.fy = X.y;
+        s.H = {H.x, H.y, H.z, H.w};
+        s.Jp = Jp;
+        s.meta = __float_as_uint(X.w);
+        return s;
     }
     static __device__ __forceinline__ St load_staged(const Stage &S, int lane)
     {
-        St s;
-        uint32_t c = S.cell[lane];
-        float2 f = S.frac[lane];
-        float4 H = S.H[lane];
-        s.ix = cell_x(c); s.iy = cell_y(c);
-        s.fx = f.x; s.fy = f.y;
-        s.H = {H.x, H.y, H.z, H.w};
-        s.Jp = S.Jp[lane];
-        s.meta = S.meta[lane];
-        return s;
+        return unpack(S.X[lane], S.H[lane], S.Jp[lane]);
     }
 
     static __device__ __forceinline__ void init_tables(Tables &T, const Consts &K, int tid, int nthr)
@@ -466,19 +473,7 @@ struct Pol32 {
         r.wy[0] = 0.5f * b0 * b0; r.wy[1] = 0.75f - b1 * b1; r.wy[2] = 0.5f * b2 * b2;
         return r;
     }
-    static __device__ __forceinline__ St load(const Parts &A, int p)
-    {
-        St s;
-        uint32_t c = A.cell[p];
-        float2 f = A.frac[p];
-        float4 H = A.H[p];
-        s.ix = cell_x(c); s.iy = cell_y(c);
-        s.fx = f.x; s.fy = f.y;
-        s.H = {H.x, H.y, H.z, H.w};
-        s.Jp = A.Jp[p];
-        s.meta = A.meta[p];
-        return s;
-    }
+    static __device__ __forceinline__ St load(const Parts &A, int p) { return unpack(A.X[p], A.H[p], A.Jp[p]); }
     static __device__ __forceinline__ void node_velocity(const icy_SimParams &P, const Consts &k, const Node &n, int gx,
                                                          int gy, double ind_x, double ind_y, float &v0, float &v1,
                                                          double &f0, double &f1, int &bin, bool contact)
@@ -583,13 +578,11 @@ struct Pol32 {
         }
         return {t.t00, t.t01, t.t01, t.t11};
     }
-    static __device__ __forceinline__ void store(const Parts &A, int p, const St &s, float jp_old, uint32_t meta_old)
+    static __device__ __forceinline__ void store(const Parts &A, int p, const St &s, float jp_old, uint32_t)
     {
-        A.cell[p] = pack_cell(s.ix, s.iy);
-        A.frac[p] = make_float2(s.fx, s.fy);
+        A.X[p] = pack_x32(s.ix, s.iy, s.fx, s.fy, s.meta);
         A.H[p] = make_float4(s.H.a00, s.H.a01, s.H.a10, s.H.a11);
         if (s.Jp != jp_old) A.Jp[p] = s.Jp;
-        if (s.meta != meta_old) A.meta[p] = s.meta;
     }
     static __device__ __forceinline__ float mass(const icy_SimParams &, const Consts &k) { return k.mass; }
     static __device__ __forceinline__ float h(const icy_SimParams &, const Consts &k) { return k.h; }
@@ -721,7 +714,7 @@ struct Pol32S : Pol32 {
         s.fy = h.fy;
         s.H = {h.H[0], h.H[1], h.H[2], h.H[3]};
         s.Jp = A.Jp[p];
-        s.meta = A.meta[p];
+        s.meta = __float_as_uint(A.X[p].w);
         v0 = h.v0;
         v1 = h.v1;
         for (int j = 0; j < 4; j++) B[j] = h.B[j];
@@ -1970,17 +1963,14 @@ __global__ void k_pack32(const icy_SimParams P, const int *perm, const int *key,
     int ix = (int)fx, iy = (int)fy;
     if (rx >= 1.0f) { rx = 0.0f; ix += 1; }
     if (ry >= 1.0f) { ry = 0.0f; iy += 1; }
-    A.cell[k] = pack_cell(ix, iy);
-    A.frac[k] = make_float2(rx, ry);
+    const int16_t *gr = (const int16_t *)((const char *)P.pts_array + P.nPtsPitch);
+    A.X[k] = pack_x32(ix, iy, rx, ry, grain_meta32(gr[i], ((const uint8_t *)P.pts_array)[i]));
     A.vel[k] = make_float2((float)row(ICM_IDX_VELX), (float)row(ICM_IDX_VELX + 1));
     A.H[k] = make_float4((float)(row(ICM_IDX_FE00) - 1.0), (float)row(ICM_IDX_FE00 + 1), (float)row(ICM_IDX_FE00 + 2),
                          (float)(row(ICM_IDX_FE00 + 3) - 1.0));
     A.Bp[k] = make_float4((float)row(ICM_IDX_BP00), (float)row(ICM_IDX_BP00 + 1), (float)row(ICM_IDX_BP00 + 2),
                           (float)row(ICM_IDX_BP00 + 3));
     A.Jp[k] = (float)row(ICM_IDX_JP_INV);
-    const uint8_t *cr = (const uint8_t *)P.pts_array;
-    const int16_t *gr = (const int16_t *)((const char *)P.pts_array + P.nPtsPitch);
-    A.meta[k] = grain_meta32(gr[i], cr[i]);
 }
 
 __global__ void k_unpack32(const icy_SimParams P, int nslots, const int *pid, const Parts32 A, int write_pq)
@@ -1992,8 +1982,9 @@ __global__ void k_unpack32(const icy_SimParams P, int nslots, const int *pid, co
     double *pts = P.pts_array;
     const size_t pp = P.nPtsPitch;
     auto row = [&](int r) -> double & { return pts[(size_t)r * pp + i]; };
-    uint32_t c = A.cell[k];
-    float2 f = A.frac[k], v = A.vel[k];
+    const float4 X = A.X[k];
+    const uint32_t c = __float_as_uint(X.z);
+    const float2 f = make_float2(X.x, X.y), v = A.vel[k];
     float4 H = A.H[k], B = A.Bp[k];
     row(ICM_IDX_POSX) = ((double)cell_x(c) + (double)f.x) * P.cellsize;
     row(ICM_IDX_POSX + 1) = ((double)cell_y(c) + (double)f.y) * P.cellsize;
@@ -2002,7 +1993,7 @@ __global__ void k_unpack32(const icy_SimParams P, int nslots, const int *pid, co
     row(ICM_IDX_FE00 + 2) = H.z; row(ICM_IDX_FE00 + 3) = 1.0 + (double)H.w;
     row(ICM_IDX_BP00) = B.x; row(ICM_IDX_BP00 + 1) = B.y; row(ICM_IDX_BP00 + 2) = B.z; row(ICM_IDX_BP00 + 3) = B.w;
     row(ICM_IDX_JP_INV) = A.Jp[k];
-    ((uint8_t *)pts)[i] = (uint8_t)meta32_crushed(A.meta[k]);
+    ((uint8_t *)pts)[i] = (uint8_t)meta32_crushed(__float_as_uint(X.w));
     if (write_pq) {
         float2 q = A.pq[k];
         row(ICM_IDX_P) = q.x;
@@ -2070,11 +2061,9 @@ __global__ void k_rebin_order(int ncells, const int *start, int *order, const in
 
 __device__ __forceinline__ void copy_slot(const Parts32 &S, int from, const Parts32 &D, int to, bool pq)
 {
-    D.cell[to] = S.cell[from];
-    D.frac[to] = S.frac[from];
+    D.X[to] = S.X[from];
     D.H[to] = S.H[from];
     D.Jp[to] = S.Jp[from];
-    D.meta[to] = S.meta[from];
     if (pq) D.pq[to] = S.pq[from];
 }
 __device__ __forceinline__ void copy_slot(const Parts64 &S, int from, const Parts64 &D, int to, bool pq)
