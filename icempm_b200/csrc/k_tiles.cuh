@@ -359,7 +359,7 @@ struct Pol64 {
         M2d F = s.F;
         s.F = {M00 * F.a00 + M01 * F.a10, M00 * F.a01 + M01 * F.a11, M10 * F.a00 + M11 * F.a10, M10 * F.a01 + M11 * F.a11};
         uint8_t cr = (uint8_t)(s.meta >> 16);
-        constitutive64(P, s.F, s.Jp, cr, grain_res((int)(int16_t)(s.meta & 0xffffu)), p_tr, q_tr);
+        constitutive64_intact_first(P, s.F, s.Jp, cr, grain_res((int)(int16_t)(s.meta & 0xffffu)), p_tr, q_tr);
         s.meta = (s.meta & 0xffffu) | ((uint32_t)cr << 16);
         redo = 0;
         return stress(P, K, s);

@@ -227,7 +227,7 @@ __host__ __device__ __forceinline__ int dp_map32(const Consts32 &k, M2f &H, floa
 // new H; rc is dp_map32's.
 struct Crushed32 { M2f H; float Jp, p, q; Tau32 tau; int rc; };
 
-__device__ __noinline__ Crushed32 crushed32(const Consts32 &k, const M2f H, const float Jp)
+static __device__ __noinline__ Crushed32 crushed32(const Consts32 &k, const M2f H, const float Jp)
 {
     Crushed32 o{H, Jp, 0.0f, 0.0f, {0.0f, 0.0f, 0.0f}, kC32_OK};
     const Inv32 v = invariants32(H, k.mu, k.kappa);
@@ -278,8 +278,8 @@ __device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTabl
 // loop.
 struct Via64 { M2f H; float Jp, p_tr, q_tr; uint32_t meta; };
 
-__device__ __noinline__ Via64 constitutive32_via64(const icy_SimParams &P, const M2f H, const float Jp_inv,
-                                                   const uint32_t meta)
+static __device__ __noinline__ Via64 constitutive32_via64(const icy_SimParams &P, const M2f H, const float Jp_inv,
+                                                          const uint32_t meta)
 {
     M2d F = {1.0 + (double)H.a00, (double)H.a01, (double)H.a10, 1.0 + (double)H.a11};
     double jp = Jp_inv, p, q;

@@ -215,6 +215,52 @@ __device__ __forceinline__ void constitutive64(const icy_SimParams &P, M2d &Fe, 
     }
 }
 
+// constitutive64 out of line, taking and returning values (a caller's hot
+// loop keeps none of the SVD's registers and no state in local memory).
+struct Cons64 { M2d F; double Jp, p, q; uint8_t crushed; };
+
+static __device__ __noinline__ Cons64 constitutive64_call(const icy_SimParams &P, const M2d F, const double Jp,
+                                                    const uint8_t crushed, const GrainRes grain)
+{
+    Cons64 o{F, Jp, 0.0, 0.0, crushed};
+    constitutive64(P, o.F, o.Jp, o.crushed, grain, o.p, o.q);
+    return o;
+}
+
+// The same update with ComputePQ's p and q of an intact particle taken from
+// invariants of b = F F^T instead of the SVD: with J = det F and
+// b - (tr b / 2) I = [[hd, b01], [b01, -hd]], the squared singular values
+// differ by 2 |(hd, b01)|, so p = -kappa/2 (J^2 - 1) and
+// q = sqrt(2) |mu/J dev(s^2)| = 2 (mu/J) sqrt(hd^2 + b01^2). An intact
+// particle found inside its failure surface this way is done (Fe and
+// Jp_inv unchanged); every other particle takes constitutive64 (SVD, the
+// failure check again, the Drucker-Prager map). The results agree with
+// constitutive64 to rounding (p, q within a few ulp); a particle within
+// that rounding of its failure surface could be judged differently.
+__device__ __forceinline__ void constitutive64_intact_first(const icy_SimParams &P, M2d &Fe, double &Jp_inv,
+                                                            uint8_t &crushed, GrainRes grain, double &p_tr,
+                                                            double &q_tr)
+{
+    if (crushed == 0) {
+        const double Je = Fe.a00 * Fe.a11 - Fe.a10 * Fe.a01;
+        const double b00 = Fe.a00 * Fe.a00 + Fe.a01 * Fe.a01, b11 = Fe.a10 * Fe.a10 + Fe.a11 * Fe.a11;
+        const double b01 = Fe.a00 * Fe.a10 + Fe.a01 * Fe.a11, hd = 0.5 * (b00 - b11);
+        const double p = -(P.kappa / 2.) * (Je * Je - 1.);
+        const double q = 2.0 * (P.mu / Je) * sqrt(hd * hd + b01 * b01);
+        if (Je > 0 && !outside_failure_surface64(P, grain, p, q)) {
+            p_tr = p;
+            q_tr = q;
+            return;
+        }
+    }
+    const Cons64 o = constitutive64_call(P, Fe, Jp_inv, crushed, grain);
+    Fe = o.F;
+    Jp_inv = o.Jp;
+    crushed = o.crushed;
+    p_tr = o.p;
+    q_tr = o.q;
+}
+
 // Quadratic B-spline weights of v2_kernel_p2g / v2_kernel_g2p
 // (gpu_implementation5.cu:185-193, 325-333): base node by truncation,
 // fx in cell units relative to the base node.
