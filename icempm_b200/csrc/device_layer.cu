@@ -71,6 +71,7 @@ struct Binning {
     int *chunk = nullptr, *tile_start = nullptr, *pid = nullptr;
     int *group_slots = nullptr, *group_base = nullptr, *gchunk = nullptr;
     int *lane_cell = nullptr, *cell_lane = nullptr;  // lane order of the cells of each tile
+    int *nbusy = nullptr;                            // tiles holding particles (1 int)
     size_t cap_pts = 0, cap_cells = 0, cap_tiles = 0, cap_slots = 0;
 };
 
@@ -89,6 +90,7 @@ struct Fused {
     // tile scheduling: measured cost and launch order per tile
     unsigned *cost = nullptr;
     int *order = nullptr;
+    int *empties = nullptr;  // the tiles without particles, for the order's empty groups
     int cost_variant = -1, cost_ntiles = -1;  // what the costs were measured on
 };
 
@@ -140,7 +142,8 @@ struct icm_ctx {
     bool pdl_next = false;
     int internal_variant = -1;
     int nslots = 0;
-    int *h_ns = nullptr;  // pinned: the slot count a re-binning reads back
+    int *h_ns = nullptr;  // pinned: the slot count and busy tiles a re-binning reads back
+    int nbusy = 0;        // tiles holding particles in the current binning
     // TMA descriptors of the three grid buffers (device copy) and what they
     // were encoded for
     CUtensorMap *d_tmap = nullptr;
@@ -263,7 +266,7 @@ static void free_fused(icm_ctx *c)
     dfree(c->fz.p32.vel); dfree(c->fz.p32.Bp); dfree(c->fz.p32.pq);
     for (int b = 0; b < 3; b++) { if (c->fz.grid[b]) cudaFree(c->fz.grid[b]); c->fz.grid[b] = nullptr; }
     dfree(c->fz.dirty);
-    dfree(c->fz.cost); dfree(c->fz.order);
+    dfree(c->fz.cost); dfree(c->fz.order); dfree(c->fz.empties);
     c->fz = Fused{};
 }
 
@@ -272,7 +275,7 @@ static void free_binning(icm_ctx *c)
     dfree(c->bin.key); dfree(c->bin.count); dfree(c->bin.cell_start); dfree(c->bin.cursor);
     dfree(c->bin.perm); dfree(c->bin.chunk); dfree(c->bin.tile_start); dfree(c->bin.pid);
     dfree(c->bin.group_slots); dfree(c->bin.group_base); dfree(c->bin.gchunk);
-    dfree(c->bin.lane_cell); dfree(c->bin.cell_lane);
+    dfree(c->bin.lane_cell); dfree(c->bin.cell_lane); dfree(c->bin.nbusy);
     c->bin = Binning{};
 }
 
@@ -291,7 +294,7 @@ static int ensure_grids(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t
     if (c->fz.form != form || c->fz.cap_nodes < nnodes || c->fz.cap_tiles < ntiles) {
         for (int b = 0; b < 3; b++) { if (c->fz.grid[b]) cudaFree(c->fz.grid[b]); c->fz.grid[b] = nullptr; }
         dfree(c->fz.dirty);
-        dfree(c->fz.cost); dfree(c->fz.order);
+        dfree(c->fz.cost); dfree(c->fz.order); dfree(c->fz.empties);
         c->fz.cost_variant = -1;
         c->fz.cap_nodes = nnodes;
         c->fz.cap_tiles = ntiles;
@@ -310,7 +313,7 @@ static int ensure_grids(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t
         // cost: a tile's two halves; order: the tiles plus at most one
         // extra CTA per tile (the second halves of split tiles)
         if ((rc = dalloc(&c->fz.dirty, 3 * ntiles)) || (rc = dalloc(&c->fz.cost, 2 * ntiles)) ||
-            (rc = dalloc(&c->fz.order, 2 * ntiles)))
+            (rc = dalloc(&c->fz.order, 2 * ntiles)) || (rc = dalloc(&c->fz.empties, ntiles)))
             return rc;
     }
     if (c->bin.cap_pts < npts || c->bin.cap_cells < ncells || c->bin.cap_tiles < ntiles) {
@@ -329,7 +332,8 @@ static int ensure_grids(icm_ctx *c, int form, size_t npts, size_t nnodes, size_t
             (rc = dalloc(&c->bin.cursor, ncells + 1)) || (rc = dalloc(&c->bin.chunk, nchunks + 1)) ||
             (rc = dalloc(&c->bin.tile_start, ntiles + 1)) || (rc = dalloc(&c->bin.group_slots, ngroups + 1)) ||
             (rc = dalloc(&c->bin.group_base, ngroups + 1)) || (rc = dalloc(&c->bin.gchunk, ngchunks + 1)) ||
-            (rc = dalloc(&c->bin.lane_cell, ncells)) || (rc = dalloc(&c->bin.cell_lane, ncells)))
+            (rc = dalloc(&c->bin.lane_cell, ncells)) || (rc = dalloc(&c->bin.cell_lane, ncells)) ||
+            (rc = dalloc(&c->bin.nbusy, 1)))
             return rc;
         c->bin.cap_pts = npts;
         c->bin.cap_cells = ncells;
@@ -420,7 +424,9 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
     }
     k_bin_order<<<(int)((ncells + 255) / 256), 256, 0, s>>>((int)ncells, c->bin.cell_start, c->bin.perm);
     ICM_LAUNCHED("k_bin_order");
-    k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start);
+    ICM_CUDA(cudaMemsetAsync(c->bin.nbusy, 0, sizeof(int), s));
+    k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start,
+                                                          c->bin.nbusy);
     ICM_LAUNCHED("k_tile_starts");
     k_lane_order<<<ntiles, 256, 0, s>>>(g.TX * g.TY, c->bin.cell_start, c->bin.lane_cell, c->bin.cell_lane);
     ICM_LAUNCHED("k_lane_order");
@@ -428,9 +434,11 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
                                                         c->bin.group_slots);
     ICM_LAUNCHED("k_group_slots");
     if ((rc = scan_ints(c, c->bin.group_slots, ngroups, c->bin.gchunk, c->bin.group_base))) return rc;
-    int nslots = 0;
+    int nslots = 0, nbusy = 0;
     ICM_CUDA(cudaMemcpyAsync(&nslots, c->bin.group_base + ngroups, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICM_CUDA(cudaMemcpyAsync(&nbusy, c->bin.nbusy, sizeof(int), cudaMemcpyDeviceToHost, s));
     ICM_CUDA(cudaStreamSynchronize(s));
+    c->nbusy = nbusy;
     if ((rc = ensure_slots(c, storage_form(c->form), (size_t)std::max(nslots, 1)))) return rc;
     if ((rc = ensure_spare(c, (size_t)std::max(nslots, 1)))) return rc;
     ICM_CUDA(cudaMemsetAsync(c->bin.pid, 0xff, sizeof(int) * (size_t)std::max(nslots, 1), s));
@@ -609,7 +617,9 @@ static int rebin_begin(icm_ctx *c, const icy_SimParams &P)
     }
     k_rebin_order<<<(int)((ncells + 255) / 256), 256, 0, s>>>((int)ncells, c->bin.cell_start, c->bin.perm, c->bin.pid);
     ICM_LAUNCHED("k_rebin_order");
-    k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start);
+    ICM_CUDA(cudaMemsetAsync(c->bin.nbusy, 0, sizeof(int), s));
+    k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start,
+                                                          c->bin.nbusy);
     ICM_LAUNCHED("k_tile_starts");
     k_lane_order<<<ntiles, 256, 0, s>>>(g.TX * g.TY, c->bin.cell_start, c->bin.lane_cell, c->bin.cell_lane);
     ICM_LAUNCHED("k_lane_order");
@@ -617,11 +627,12 @@ static int rebin_begin(icm_ctx *c, const icy_SimParams &P)
                                                         c->bin.group_slots);
     ICM_LAUNCHED("k_group_slots");
     if ((rc = scan_ints(c, c->bin.group_slots, ngroups, c->bin.gchunk, c->bin.group_base))) return rc;
-    if (!c->h_ns && cudaMallocHost((void **)&c->h_ns, sizeof(int)) != cudaSuccess) {
+    if (!c->h_ns && cudaMallocHost((void **)&c->h_ns, 2 * sizeof(int)) != cudaSuccess) {
         c->h_ns = nullptr;
         return icm::fail(ICM_ERR_NOMEM, "re-binning: pinned slot count");
     }
     ICM_CUDA(cudaMemcpyAsync(c->h_ns, c->bin.group_base + ngroups, sizeof(int), cudaMemcpyDeviceToHost, s));
+    ICM_CUDA(cudaMemcpyAsync(c->h_ns + 1, c->bin.nbusy, sizeof(int), cudaMemcpyDeviceToHost, s));
     return ICM_OK;
 }
 
@@ -636,7 +647,8 @@ static int rebin_finish(icm_ctx *c, const icy_SimParams &P, bool keep_pq)
     const Consts32 K32 = make_consts32(P);
     const Pol64::Consts K64{0};
     int rc;
-    const int ns_new = *c->h_ns;
+    const int ns_new = c->h_ns[0];
+    c->nbusy = c->h_ns[1];
     if ((size_t)ns_new > c->fz.spare_cap) {
         // the spare set must hold the new layout; grow it (contents of the
         // current set are untouched)
@@ -760,11 +772,14 @@ static int tile_order(icm_ctx *c, int ntiles, const int *&order, int &nlaunch)
     if (ntiles > kMaxOrderTiles) return ICM_OK;
     const int max_split = std::min(std::max(c->split_max, 0), ntiles);
     k_tile_order<<<1, kOrderThreads, sizeof(int) * (size_t)ntiles, c->stream>>>(
-        ntiles, c->fz.cost, c->bin.tile_start, max_split, (float)c->split_ratio, c->fz.order);
+        ntiles, c->fz.cost, c->bin.tile_start, max_split, (float)c->split_ratio, c->fz.order, c->fz.empties);
     ICM_LAUNCHED("k_tile_order");
     c->pdl_next = false;  // the substep reads the order before its dependency wait
     order = c->fz.order;
-    nlaunch = ntiles + max_split;
+    // the busy tiles, the second halves of at most max_split split tiles and
+    // the groups of tiles without particles (entries past the used ones are -1)
+    const int nbusy = std::min(std::max(c->nbusy, 0), ntiles);
+    nlaunch = nbusy + max_split + (ntiles - nbusy + kEmptyPerCta - 1) / kEmptyPerCta;
     return ICM_OK;
 }
 
@@ -813,6 +828,8 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
     R.cost = c->fz.cost;
     int nlaunch = ntiles;
     if ((rc = tile_order(c, ntiles, R.order, nlaunch))) return rc;
+    R.empties = c->fz.empties;
+    R.nempty = ntiles - std::min(std::max(c->nbusy, 0), ntiles);
     if ((rc = ensure_tmaps(c, P))) return rc;
     R.tmap = c->tmap_ok ? c->d_tmap : nullptr;
 
@@ -877,6 +894,7 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
             if ((rc = rebin_internal(c, P, c->internal_pq || any_pq))) return rc;
             R.group_base = c->bin.group_base;
             if ((rc = tile_order(c, ntiles, R.order, nlaunch))) return rc;
+            R.nempty = ntiles - std::min(std::max(c->nbusy, 0), ntiles);
         }
     }
     p->SimulationStep += n;

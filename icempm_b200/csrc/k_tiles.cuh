@@ -191,6 +191,9 @@ struct TileRun {
     // TMA descriptors of the three grid buffers in global memory, or null
     // (ensembles; a single run passes them as a kernel parameter)
     const CUtensorMap *tmap;
+    // the tiles without particles, for the order's empty groups
+    const int *empties;
+    int nempty;
 };
 
 // the TMA descriptors of the three grid buffers, as a kernel parameter
@@ -206,8 +209,11 @@ constexpr int kErrTmaTimeout = 4;
 // count field); its particles beyond that were not advanced
 constexpr int kErrCellOverflow = 8;
 
-// launch-order entries of the fused kernel (k_tile_order)
-constexpr int kTileMask = (1 << 29) - 1, kSplitBit = 1 << 29, kHalfBit = 1 << 30;
+// launch-order entries of the fused kernel (k_tile_order): a tile, or a
+// half of a split tile, or a group of kEmptyPerCta tiles without particles
+// (kEmptyBit | group index into TileRun::empties)
+constexpr int kTileMask = (1 << 28) - 1, kEmptyBit = 1 << 28, kSplitBit = 1 << 29, kHalfBit = 1 << 30;
+constexpr int kEmptyPerCta = 8;
 constexpr int kTmaPolls = 1 << 22;
 
 // Copies the (RX x RY)-node region at node (rx0, ry0) of one grid buffer
@@ -930,6 +936,19 @@ __device__ __forceinline__ int group_of(int j, int warp, int nwarps, int part)
     return part == 0 ? m : 2 * m + (part - 1);
 }
 
+// Whether a node of tile t's (TX+4) x (TY+4) region lies inside the
+// indenter's circle.
+template <int TX, int TY>
+__device__ __forceinline__ bool region_touches_indenter(const icy_SimParams &P, const TileRun &R, int t)
+{
+    const int rx0 = (t % R.ntx) * TX - 1, ry0 = (t / R.ntx) * TY - 1;
+    const double h = P.cellsize, r = sqrt(P.IndRSq);
+    const double lox = rx0 * h, hix = (rx0 + TX + 3) * h, loy = ry0 * h, hiy = (ry0 + TY + 3) * h;
+    const double cx = fmin(fmax(R.ind_x, lox), hix), cy = fmin(fmax(R.ind_y, loy), hiy);
+    const double dx = cx - R.ind_x, dy = cy - R.ind_y;
+    return dx * dx + dy * dy <= r * r;
+}
+
 // Dynamic shared memory of one CTA (host and kernel use the same layout):
 // the warps' P2G regions (none in the final launch), then Pol::kStages
 // staging rounds per warp.
@@ -1063,11 +1082,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     // can any node of the region touch the indenter?
     bool contact_possible = false;
     if (MODE != kModeP2GOnly) {
-        double h = P.cellsize, r = sqrt(P.IndRSq);
-        double lox = rx0 * h, hix = (rx0 + RX - 1) * h, loy = ry0 * h, hiy = (ry0 + RY - 1) * h;
-        double cx = fmin(fmax(R.ind_x, lox), hix), cy = fmin(fmax(R.ind_y, loy), hiy);
-        double dx = cx - R.ind_x, dy = cy - R.ind_y;
-        contact_possible = dx * dx + dy * dy <= r * r;
+        contact_possible = region_touches_indenter<TX, TY>(P, R, t);
         if (contact_possible) {
             for (int k = tid; k < 2 * P.n_indenter_subdivisions; k += nthr) s_bins[k] = 0.0;
             if (tid == 0) { s_tot[0] = 0.0; s_tot[1] = 0.0; s_contact = 0; }
@@ -1448,6 +1463,74 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
     }
 }
 
+// Tiles without particles, kEmptyPerCta of them per CTA (an empty group of
+// the launch order). Each one's nodes in the next-but-one buffer are zeroed
+// where its dirty flag says so, and a tile that holds mass and that the
+// indenter can reach adds the reaction of its own nodes (the grid update's
+// contact, gpu_implementation5.cu:245-271) to the force bins with global
+// FP64 atomics. The group's flags are read at once, after the wait for the
+// previous substep, so that the latency of the loads is paid once per CTA.
+template <class Pol, int TX, int TY, int MODE>
+__device__ __forceinline__ void empty_group(const icy_SimParams &P, const typename Pol::Consts &K, const TileRun &R,
+                                            const int grp)
+{
+    using Node = typename Pol::Node;
+    using real = typename Pol::real;
+    __shared__ int s_et[kEmptyPerCta];
+    __shared__ uint8_t s_ez[kEmptyPerCta], s_ec[kEmptyPerCta];
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (tid < kEmptyPerCta) {
+        const int i = grp * kEmptyPerCta + tid;
+        int t = -1;
+        uint8_t z = 0, c = 0;
+        if (i < R.nempty) {
+            t = R.empties[i];
+            z = (MODE == kModeFull) ? R.dirty[R.bufC][t] : 0;
+            c = (R.dirty[R.bufA][t] && region_touches_indenter<TX, TY>(P, R, t)) ? 1 : 0;
+        }
+        s_et[tid] = t;
+        s_ez[tid] = z;
+        s_ec[tid] = c;
+    }
+    __syncthreads();
+    const int GX = P.GridX, GY = P.GridY;
+    for (int j = 0; j < kEmptyPerCta; j++) {
+        const int t = s_et[j];
+        if (t < 0) continue;
+        const int x0 = (t % R.ntx) * TX, y0 = (t / R.ntx) * TY;
+        if (s_ez[j]) {
+            Node *gC = (Node *)R.grid[R.bufC];
+            for (int k = tid; k < TX * TY; k += nthr) {
+                const int gx = x0 + k % TX, gy = y0 + k / TX;
+                if (gx < GX && gy < GY) node_zero(gC, (size_t)gy * GX + gx);
+            }
+        }
+        if (s_ec[j]) {
+            const Node *gA = (const Node *)R.grid[R.bufA];
+            for (int k = tid; k < TX * TY; k += nthr) {
+                const int gx = x0 + k % TX, gy = y0 + k / TX;
+                if (gx >= GX || gy >= GY) continue;
+                real v0, v1;
+                double f0 = 0, f1 = 0;
+                int bin;
+                Pol::node_velocity(P, K, gA[(size_t)gy * GX + gx], gx, gy, R.ind_x, R.ind_y, v0, v1, f0, f1, bin, true);
+                if (bin >= 0) {
+                    atomicAdd(&R.bins[2 * bin], f0);
+                    atomicAdd(&R.bins[2 * bin + 1], f1);
+                    if (R.force_slot) {
+                        atomicAdd(&R.force_slot[0], f0);
+                        atomicAdd(&R.force_slot[1], f1);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();  // every thread's zeroing is done before the flags clear
+    if (tid < kEmptyPerCta && s_et[tid] >= 0 && s_ez[tid]) R.dirty[R.bufC][s_et[tid]] = 0;
+}
+
 // One launch = one substep over all tiles, one CTA per tile. Tile costs are
 // uneven (indenter contact, crushed particles redone in FP64, occupancy), so
 // CTA i takes tile order[i] -- the tiles sorted by the cost measured in
@@ -1469,6 +1552,11 @@ __global__ void __maxnreg__(Pol::kMaxRegs) k_tile_substep(const __grid_constant_
         code = (int)blockIdx.x < ntiles ? (int)blockIdx.x : -1;
     }
     if (code < 0) return;
+    if (code & kEmptyBit) {
+        // the prologue (P2G of the current state) has nothing to do there
+        if (MODE != kModeP2GOnly) empty_group<Pol, TX, TY, MODE>(P, K, R, code & kTileMask);
+        return;
+    }
     const int t = code & kTileMask;
     const int part = (code & kSplitBit) ? ((code & kHalfBit) ? 2 : 1) : 0;
     if (MODE == kModeFull && threadIdx.x == 0) s_clock = clock64();
@@ -1650,22 +1738,23 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *tmp, int &total)
     return before;
 }
 
-// Tile order by descending cost (one CTA, n <= kMaxOrderTiles): a
-// counting sort on the cost quantised to kOrderLevels levels of the
-// largest cost. Inside a level the order is the order in which threads
-// claim places; nothing depends on it, since a substep's result does not
-// depend on the order its CTAs run in. A tile's cost is
-// cost[t] + cost[n + t] (its halves when it ran split); a tile without
-// particles (whose cost may be one measured before a re-binning emptied
-// it) counts as 0 and sorts last. The first S tiles of the order are split,
-// S = the number of tiles whose cost exceeds ratio times the mean over
-// tiles holding particles, at most max_split: their two halves lead the
-// order (two CTAs each), then the other tiles; the order has n + max_split
-// entries, the unused ones -1. Dynamic shared memory: n ints.
+// Launch order of the fused substep (one CTA, n <= kMaxOrderTiles): the
+// tiles holding particles by descending cost, then the tiles without
+// particles in groups of kEmptyPerCta (one CTA each, entries kEmptyBit |
+// group, the tiles listed in empties). The cost order is a counting sort on
+// the cost quantised to kOrderLevels levels of the largest cost; inside a
+// level the order is the order in which threads claim places, which no
+// result depends on (a substep's result does not depend on the order its
+// CTAs run in). A tile's cost is cost[t] + cost[n + t] (its halves when it
+// ran split). The first S tiles are split, S = the number of tiles whose
+// cost exceeds ratio times the mean over tiles holding particles, at most
+// max_split: their two halves lead the order (two CTAs each). The order has
+// n + max_split entries, the unused ones -1; a launch needs its first
+// busy + S + ceil((n - busy) / kEmptyPerCta). Dynamic shared memory: n ints.
 constexpr int kOrderLevels = kOrderThreads;
 
 __global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsigned *cost, const int *tile_start,
-                                                              int max_split, float ratio, int *order)
+                                                              int max_split, float ratio, int *order, int *empties)
 {
     extern __shared__ int s_sorted[];
     __shared__ int s_off[kOrderLevels];
@@ -1682,37 +1771,37 @@ __global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsig
         s_over = 0;
     }
     __syncthreads();
+    auto busy_tile = [&](int i) { return tile_start[i + 1] > tile_start[i]; };
     auto tile_cost = [&](int i) -> unsigned {
-        if (tile_start[i + 1] <= tile_start[i]) return 0u;
         const unsigned long long cc = (unsigned long long)cost[i] + cost[n + i];
         return cc > 0xffffffffull ? 0xffffffffu : (unsigned)cc;
     };
     unsigned long long sum = 0;
     unsigned mx = 0;
     int busy = 0;
-    for (int i = tid; i < n; i += blockDim.x) {
-        const unsigned c = tile_cost(i);
-        if (tile_start[i + 1] > tile_start[i]) {
+    for (int i = tid; i < n; i += blockDim.x)
+        if (busy_tile(i)) {
+            const unsigned c = tile_cost(i);
             sum += c;
             busy++;
+            mx = max(mx, c);
         }
-        mx = max(mx, c);
-    }
     atomicAdd(&s_sum, sum);
     atomicAdd(&s_busy, busy);
     atomicMax(&s_max, mx);
     __syncthreads();
-    const unsigned cmax = s_max;
-    // level kOrderLevels - 1 holds the heaviest tiles, level 0 the empty ones
-    auto level = [&](unsigned c) -> int {
-        return c == 0u ? 0 : 1 + (int)((unsigned long long)c * (kOrderLevels - 2) / cmax);
+    const unsigned cmax = max(s_max, 1u);
+    const int nbusy = s_busy;
+    // busy tiles take levels 1 .. kOrderLevels - 1 (the heaviest the top
+    // one), tiles without particles level 0
+    auto level = [&](int i) -> int {
+        return busy_tile(i) ? 1 + (int)((unsigned long long)tile_cost(i) * (kOrderLevels - 2) / cmax) : 0;
     };
-    const double thr = s_busy > 0 ? (double)ratio * (double)s_sum / (double)s_busy : 1e300;
+    const double thr = nbusy > 0 ? (double)ratio * (double)s_sum / (double)nbusy : 1e300;
     int over = 0;
     for (int i = tid; i < n; i += blockDim.x) {
-        const unsigned c = tile_cost(i);
-        atomicAdd(&s_off[level(c)], 1);
-        over += (double)c > thr;
+        atomicAdd(&s_off[level(i)], 1);
+        over += busy_tile(i) && (double)tile_cost(i) > thr;
     }
     atomicAdd(&s_over, over);
     __syncthreads();
@@ -1726,15 +1815,19 @@ __global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsig
         s_off[b] = before;
     }
     __syncthreads();
-    for (int i = tid; i < n; i += blockDim.x) s_sorted[atomicAdd(&s_off[level(tile_cost(i))], 1)] = i;
+    for (int i = tid; i < n; i += blockDim.x) s_sorted[atomicAdd(&s_off[level(i)], 1)] = i;
     __syncthreads();
-    const int S = min(min(s_over, max_split), n);
+    const int S = min(min(s_over, max_split), nbusy);
+    const int nempty = n - nbusy, ngroups = (nempty + kEmptyPerCta - 1) / kEmptyPerCta;
+    for (int i = tid; i < nempty; i += blockDim.x) empties[i] = s_sorted[nbusy + i];
     for (int i = tid; i < n + max_split; i += blockDim.x) {
         int v = -1;
         if (i < 2 * S) {
             v = s_sorted[i >> 1] | kSplitBit | ((i & 1) ? kHalfBit : 0);
-        } else if (i < n + S) {
+        } else if (i < nbusy + S) {
             v = s_sorted[i - S];
+        } else if (i < nbusy + S + ngroups) {
+            v = (i - nbusy - S) | kEmptyBit;
         }
         order[i] = v;
     }
@@ -1890,10 +1983,13 @@ __device__ __forceinline__ int slot_of(int q, const int *perm, const int *key, c
     return slot_in_cell(k, q - cell_start[k], cell_lane, group_base);
 }
 
-__global__ void k_tile_starts(int ntiles, int cells_per_tile, const int *cell_start, int *tile_start)
+// tile_start[t] = first particle of tile t; *nbusy (zeroed by the caller)
+// counts the tiles holding particles
+__global__ void k_tile_starts(int ntiles, int cells_per_tile, const int *cell_start, int *tile_start, int *nbusy)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t <= ntiles) tile_start[t] = cell_start[t * cells_per_tile];
+    if (t < ntiles && cell_start[(t + 1) * cells_per_tile] > cell_start[t * cells_per_tile]) atomicAdd(nbusy, 1);
 }
 
 __device__ __forceinline__ uint32_t read_meta(const icy_SimParams &P, int i)
