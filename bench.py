@@ -405,6 +405,12 @@ def main():
                 d["roofline"] = {"achieved": a2, "frac": a2 / hbm, "from": "step time (4 launches per substep)"}
             extra[key] = d
             mm.gpu.close()
+        mc = make(im.FORM_FP32_COMPENSATED, tile)
+        msc, _ = timed(mc, k2, 1, args.substeps)
+        extra["fp32_compensated"] = {"value": job_rate(world, n * args.substeps * k2, rank_max(sum(msc) / 1e3)),
+                                     "ms_per_step": sum(msc) / k2, "steps": k2,
+                                     "avg_launch_us": sum(msc) / k2 / args.substeps * 1e3}
+        mc.gpu.close()
         extra["speedup_fp32_vs_fp64_stepwise"] = value / extra["fp64_stepwise"]["value"]
         extra["speedup_fp32_vs_fp64_fused"] = value / extra["fp64_fused"]["value"]
 
@@ -426,10 +432,22 @@ def main():
 
         # the FP32 form's state against the FP64 fused form's after 1, 10 and
         # 100 substeps from the same initial state
-        early = {}
+        early, early_c = {}, {}
         pm = int(p0.nPtsPitch)
-        pair = [make(im.FORM_FP64, tile64, threads64), make(im.FORM_FP32, tile)]
+        pair = [make(im.FORM_FP64, tile64, threads64), make(im.FORM_FP32, tile),
+                make(im.FORM_FP32_COMPENSATED, tile)]
         done = 0
+
+        def state_err(a, b):
+            dfe = np.abs(b.Fe - a.Fe).max(axis=0)
+            strain = np.abs(a.Fe - np.array([1.0, 0.0, 0.0, 1.0])[:, None]).max()
+            return {
+                "x_max_err_h": float(np.abs(b.pos - a.pos).max() / p0.cellsize),
+                "v_rel_err": float(np.abs(b.vel - a.vel).max() / max(np.abs(a.vel).max(), 1e-30)),
+                "Fe_err_rel_to_max_strain": float(dfe.max() / max(strain, 1e-30)),
+                "Fe_err_p99_rel_to_max_strain": float(np.percentile(dfe, 99) / max(strain, 1e-30)),
+                "Jp_inv_max_abs_err": float(np.abs(b.Jp_inv - a.Jp_inv).max()),
+            }
         for target in (1, 10, 100):
             bufs = []
             for mm in pair:
@@ -438,22 +456,15 @@ def main():
                 mm.gpu.synchronize()
                 bufs.append(im.SoA(mm.gpu.tmp_transfer_buffer.copy(), pm, n))
             done = target
-            a, b = bufs
-            dfe = np.abs(b.Fe - a.Fe).max(axis=0)
-            strain = np.abs(a.Fe - np.array([1.0, 0.0, 0.0, 1.0])[:, None]).max()
-            early[str(target)] = {
-                "x_max_err_h": float(np.abs(b.pos - a.pos).max() / p0.cellsize),
-                "v_rel_err": float(np.abs(b.vel - a.vel).max() / max(np.abs(a.vel).max(), 1e-30)),
-                "Fe_err_rel_to_max_strain": float(dfe.max() / max(strain, 1e-30)),
-                "Fe_err_p99_rel_to_max_strain": float(np.percentile(dfe, 99) / max(strain, 1e-30)),
-                "Jp_inv_max_abs_err": float(np.abs(b.Jp_inv - a.Jp_inv).max()),
-            }
+            early[str(target)] = state_err(bufs[0], bufs[1])
+            early_c[str(target)] = state_err(bufs[0], bufs[2])
         for mm in pair:
             mm.gpu.close()
 
         redo_frame = 0
-        for form in (im.FORM_FP64, im.FORM_FP32, im.FORM_FP64_STEPWISE):
-            mm = make(form, tile64 if form != im.FORM_FP32 else tile, threads64 if form != im.FORM_FP32 else None)
+        for form in (im.FORM_FP64, im.FORM_FP32, im.FORM_FP64_STEPWISE, im.FORM_FP32_COMPENSATED):
+            f32_like = form in (im.FORM_FP32, im.FORM_FP32_COMPENSATED)
+            mm = make(form, tile if f32_like else tile64, None if f32_like else threads64)
             mm.gpu.run_substeps(mm.prms, nsub)
             if form == im.FORM_FP32:
                 redo_frame = mm.gpu.fp64_redo_count()
@@ -463,12 +474,13 @@ def main():
             mm.gpu.cuda_transfer_from_device()
             mm.gpu.synchronize()
             res[form] = (hist, mm.gpu.tmp_transfer_buffer.copy(), mm.gpu.error_code)
-            if form != im.FORM_FP64_STEPWISE:
+            if form not in (im.FORM_FP64_STEPWISE, im.FORM_FP32_COMPENSATED):
                 late[im.FORM_NAMES[form]] = late_launch_us(mm)
             mm.gpu.close()
         h64, s64, e64 = res[im.FORM_FP64]
         h32, s32, e32 = res[im.FORM_FP32]
         hsw, ssw, esw = res[im.FORM_FP64_STEPWISE]
+        hc, sc_, ec = res[im.FORM_FP32_COMPENSATED]
         f64 = np.hypot(h64[:, 0], h64[:, 1])
         f32 = np.hypot(h32[:, 0], h32[:, 1])
         fsw = np.hypot(hsw[:, 0], hsw[:, 1])
@@ -509,6 +521,7 @@ def main():
                 mm.gpu.close()
             spread[f"{amp:g}"] = {k: sorted(r[k] for r in runs) for k in runs[0]}
         e32f = frame_errors(f32, pos(s32))
+        e32c = frame_errors(np.hypot(hc[:, 0], hc[:, 1]), pos(sc_))
 
         def rank_in_spread(err):
             """For each measure: the share of the perturbed FP64 runs (all
@@ -532,7 +545,11 @@ def main():
                 "seeds": SPREAD_SEEDS, "errors_sorted_by_amplitude": spread,
                 "what": "FP64 fused frames from Fe + a N(0,1) (seeded), against the unperturbed FP64 frame"},
             "fp64_vs_fp64_stepwise": frame_errors(fsw, pos(ssw)),
-            "error_flags": [int(e64), int(e32), int(esw)],
+            "fp32_compensated": {
+                "what": "FP32 form with compensated (Kahan) per-cell momentum sums",
+                "state_err_after_substeps": early_c, "frame": e32c,
+                "share_of_fp64_spread_at_least_as_large": rank_in_spread(e32c)},
+            "error_flags": [int(e64), int(e32), int(esw), int(ec)],
             "late_frame_us_per_launch": late,
             "fp64_redo_per_substep": redo_frame / nsub,
             "stray_particle_substeps": {"fp64": strays.get(im.FORM_FP64), "fp32": strays.get(im.FORM_FP32)},

@@ -33,8 +33,9 @@ FORM_FP64_STEPWISE = 0
 FORM_FP64 = 1
 FORM_FP32 = 2
 FORM_FP32_SURROGATE = 3
+FORM_FP32_COMPENSATED = 4
 FORM_NAMES = {FORM_FP64_STEPWISE: "fp64-stepwise", FORM_FP64: "fp64", FORM_FP32: "fp32",
-              FORM_FP32_SURROGATE: "fp32-surrogate"}
+              FORM_FP32_SURROGATE: "fp32-surrogate", FORM_FP32_COMPENSATED: "fp32-compensated"}
 
 # tile variants of the fused forms (nodes)
 TILE_VARIANTS = {0: (16, 8), 1: (16, 16), 2: (32, 8), 3: (32, 16)}
@@ -631,4 +632,4 @@ def save_pq_host(prms: SimParams, soa: np.ndarray, outputDirectory: str) -> str:
 __all__ = ["SimParams", "BlockDesc", "GPU_Implementation5", "Model", "SoA", "make_block", "pitch_elems", "library",
            "SnapshotManager", "repitch_soa", "load_raw_points_host", "save_snapshot_host", "read_snapshot_host",
            "save_pq_host",
-           "FORM_FP64_STEPWISE", "FORM_FP64", "FORM_FP32", "FORM_FP32_SURROGATE", "FORM_NAMES", "TILE_VARIANTS", "LIB_PATH"]
+           "FORM_FP64_STEPWISE", "FORM_FP64", "FORM_FP32", "FORM_FP32_SURROGATE", "FORM_FP32_COMPENSATED", "FORM_NAMES", "TILE_VARIANTS", "LIB_PATH"]

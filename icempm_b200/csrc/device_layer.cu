@@ -158,7 +158,11 @@ struct icm_ctx {
 // ------------------------------------------------------------ helpers
 
 // the internal storage of a form: the surrogate form keeps FP32 state
-static int storage_form(int form) { return form == ICM_FORM_FP32_SURROGATE ? ICM_FORM_FP32 : form; }
+// the particle layout a form keeps on the device (the FP32 variants share the FP32 one)
+static int storage_form(int form)
+{
+    return (form == ICM_FORM_FP32_SURROGATE || form == ICM_FORM_FP32_COMPENSATED) ? ICM_FORM_FP32 : form;
+}
 
 static int check_params(icm_ctx *c, const icy_SimParams *p)
 {
@@ -863,8 +867,9 @@ static int run_fused(icm_ctx *c, icy_SimParams *p, int n)
                 K.harvest_n = c->d_harvest_n;
                 K.harvest_cap = c->harvest_cap;
             }
-            r = (c->form == ICM_FORM_FP32_SURROGATE) ? launch_variant<Pol32S>(c, mode, nlaunch, P, K, c->fz.p32, R)
-                                                     : launch_variant<Pol32>(c, mode, nlaunch, P, K, c->fz.p32, R);
+            r = (c->form == ICM_FORM_FP32_SURROGATE)     ? launch_variant<Pol32S>(c, mode, nlaunch, P, K, c->fz.p32, R)
+                : (c->form == ICM_FORM_FP32_COMPENSATED) ? launch_variant<Pol32C>(c, mode, nlaunch, P, K, c->fz.p32, R)
+                                                         : launch_variant<Pol32>(c, mode, nlaunch, P, K, c->fz.p32, R);
         }
         if (e1) ICM_CUDA(cudaEventRecord(e1, c->stream));
         return r;
@@ -991,7 +996,7 @@ extern "C" int icm_destroy(icm_ctx *c)
 extern "C" int icm_set_form(icm_ctx *c, int form)
 {
     if (!c) return icm::fail(ICM_ERR_ARG, "null context");
-    if (form < ICM_FORM_FP64_STEPWISE || form > ICM_FORM_FP32_SURROGATE) return icm::fail(ICM_ERR_ARG, "unknown form");
+    if (form < ICM_FORM_FP64_STEPWISE || form > ICM_FORM_FP32_COMPENSATED) return icm::fail(ICM_ERR_ARG, "unknown form");
     if (form == c->form) return ICM_OK;
     if (c->d_pts) {
         int rc = ensure_ref(c);

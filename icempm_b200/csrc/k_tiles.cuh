@@ -168,6 +168,58 @@ template <> struct CellSums<float> {
     }
 };
 
+// The FP32 per-cell sums with compensated (Kahan) momentum accumulation:
+// each momentum sum s carries the low-order part c that its additions lost,
+// updated as y = p + c, t = s + y, c = y - (t - s), s = t (the differences
+// as multiply-adds by -1, one rounding each); the flush adds s + c. The
+// masses are sums of positive terms and are added plainly.
+struct CellSumsComp {
+    CellSums<float> b;
+    float2 cxy[9];
+    __device__ __forceinline__ void zero()
+    {
+        b.zero();
+#pragma unroll
+        for (int q = 0; q < 9; q++) cxy[q] = make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ void add(const float wx[3], const float wy[3], float mass, float c0, float c1, float S00,
+                                        float S01, float S10, float S11)
+    {
+        const float2 c = make_float2(c0, c1), s0 = make_float2(S00, S10), s1 = make_float2(S01, S11);
+        const float2 wx01 = make_float2(wx[0], wx[1]), m1 = bcast2(-1.0f);
+        float2 wyy[3];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            wyy[j] = bcast2(wy[j]);
+            const float2 mw = __fmul2_rn(bcast2(mass), wyy[j]);
+            b.m01[j] = __ffma2_rn(mw, wx01, b.m01[j]);
+            b.m2[j] = fmaf(mw.x, wx[2], b.m2[j]);
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            const float2 u = i == 0 ? c : __ffma2_rn(bcast2((float)i), s0, c);
+            const float2 wxx = bcast2(wx[i]);
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int q = i * 3 + j;
+                const float2 uj = j == 0 ? u : __ffma2_rn(bcast2((float)j), s1, u);
+                const float2 y = __fadd2_rn(__fmul2_rn(__fmul2_rn(wxx, wyy[j]), uj), cxy[q]);
+                const float2 t = __fadd2_rn(b.xy[q], y);
+                cxy[q] = __ffma2_rn(__ffma2_rn(b.xy[q], m1, t), m1, y);  // y - (t - s)
+                b.xy[q] = t;
+            }
+        }
+    }
+    __device__ __forceinline__ void flush(float4 &ac, int i, int j) const
+    {
+        float4 v = ac;
+        const int q = i * 3 + j;
+        const float2 s = __fadd2_rn(make_float2(v.x, v.y), __fadd2_rn(b.xy[q], cxy[q]));
+        const float mm = i == 2 ? b.m2[j] : (i == 0 ? b.m01[j].x : b.m01[j].y);
+        ac = make_float4(s.x, s.y, v.z + mm, v.w);
+    }
+};
+
 struct TileRun {
     int ntx, nty;
     const int *tile_start;   // ntiles + 1
@@ -290,6 +342,7 @@ struct Pol64 {
     using Node = Node64;
     using Acc = Acc64;
     using Parts = Parts64;
+    using Sums = CellSums<double>;
     struct Consts { int dummy; };
     struct Tables { int dummy; };
     struct St { double x, y; M2d F; double Jp; uint32_t meta; };
@@ -423,6 +476,7 @@ struct Pol32 {
     using Node = float4;
     using Acc = float4;
     using Parts = Parts32;
+    using Sums = CellSums<float>;
     using Consts = Consts32;
     using Tables = GrainTables32;
     struct St { int ix, iy; float fx, fy; M2f H; float Jp; uint32_t meta; };
@@ -771,6 +825,15 @@ struct Pol32S : Pol32 {
         fp64 += o.fp64;
         return stress(P, k, s);
     }
+};
+
+// FP32 strain form with compensated per-cell momentum sums (CellSumsComp):
+// the same arithmetic as Pol32 otherwise. The 18 compensation terms need
+// registers beyond the FP32 form's 128, so this form runs three 128-thread
+// CTAs per SM.
+struct Pol32C : Pol32 {
+    using Sums = CellSumsComp;
+    static constexpr int kMaxRegs = 168;
 };
 
 // ------------------------------------------------------- grid node access
@@ -1216,7 +1279,7 @@ __device__ __forceinline__ void tile_body(const icy_SimParams &P, const typename
         next_item(a == 0 ? k : qk[a - 1], a == 0 ? r : qr[a - 1], qk[a], qr[a]);
         if (a < kStages - 2) issue(qk[a], qr[a], a + 1);
     }
-    CellSums<real> sums;
+    typename Pol::Sums sums;
     while (k < ng_w) {
         const int nk = qk[0], nr = qr[0];
         issue(qk[kStages - 2], qr[kStages - 2], (cur + kStages - 1) % kStages);

@@ -46,7 +46,8 @@ enum {
     ICM_FORM_FP64_STEPWISE = 0, /* reference structure: reset, P2G, update, G2P launches per substep, FP64 */
     ICM_FORM_FP64 = 1,          /* fused tile substep, FP64 reference form */
     ICM_FORM_FP32 = 2,          /* fused tile substep, FP32 strain form */
-    ICM_FORM_FP32_SURROGATE = 3 /* FP32 form with the learned Drucker-Prager projection (icm_set_surrogate) */
+    ICM_FORM_FP32_SURROGATE = 3, /* FP32 form with the learned Drucker-Prager projection (icm_set_surrogate) */
+    ICM_FORM_FP32_COMPENSATED = 4 /* FP32 form with compensated (Kahan) per-cell momentum sums; single runs */
 };
 
 typedef struct icm_ctx icm_ctx;

@@ -85,19 +85,24 @@ def test_fp64_forms_match_oracle(form, tile, n):
     assert m.prms.indenter_x == q.indenter_x
 
 
+FP32_FORMS = [im.FORM_FP32, im.FORM_FP32_COMPENSATED]
+
+
+@pytest.mark.parametrize("form", FP32_FORMS)
 @pytest.mark.parametrize("tile", [0, 1, 3])
-def test_fp32_one_substep_all_branches(tile):
+def test_fp32_one_substep_all_branches(tile, form):
     """One substep from a perturbed state (crushed particles, Jp_inv != 1,
-    sheared Fe): every branch of the FP32 strain form against the oracle."""
+    sheared Fe): every branch of the FP32 strain form (plain and with
+    compensated per-cell momentum sums) against the oracle."""
     p = params(96, 48, dim=0.75, dt=2e-6)
     soa = scene(p, cells=(48, 12), seed=5, ind_y=0.05, perturb=2e-2, vel=0.05, crushed_frac=0.5, jp_spread=0.02)
-    m = gpu_model(p, soa, im.FORM_FP32, tile)
+    m = gpu_model(p, soa, form, tile)
     m.gpu.run_substeps(m.prms, 1)
     got = gpu_state(m)
     q, ref, bins, err, hist = oracle_run(p, soa, 1)
     e = compare_states(p, got, ref, soa)
     n = p.nPts
-    print("fp32 1 substep", tile, e, "redo", m.gpu.fp64_redo_count(),
+    print(im.FORM_NAMES[form], "1 substep", tile, e, "redo", m.gpu.fp64_redo_count(),
           "crushed", int(im.SoA(ref, p.nPtsPitch, n).crushed.sum()))
     assert e["crushed_mismatch"] <= max(2, n // 1000)
     assert e["grain_mismatch"] == 0
@@ -110,16 +115,17 @@ def test_fp32_one_substep_all_branches(tile):
     assert max_rel(m.gpu.force_history(1), hist) < 1e-4
 
 
+@pytest.mark.parametrize("form", FP32_FORMS)
 @pytest.mark.parametrize("tile", [1, 3])
-def test_fp32_indentation_tracks_oracle(tile):
+def test_fp32_indentation_tracks_oracle(tile, form):
     """200 substeps of a block pushed by the indenter (smooth state): the FP32
-    form stays within 1e-3 h of the FP64 oracle."""
+    forms stay within 1e-3 h of the FP64 oracle."""
     p = params(96, 48, dim=0.75, dt=2e-6)
     soa = scene(p, cells=(48, 12), seed=3, ind_y=0.05)
     S = im.SoA(soa, p.nPtsPitch, p.nPts)
     p.indenter_x = p.indenter_x_initial = S.pos[0].min() - 0.15 + 2 * p.cellsize  # 2 cells of overlap
     n = 200
-    m = gpu_model(p, soa, im.FORM_FP32, tile)
+    m = gpu_model(p, soa, form, tile)
     m.gpu.run_substeps(m.prms, n)
     got = gpu_state(m)
     q, ref, bins, err, hist = oracle_run(p, soa, n, threads=4)
@@ -128,7 +134,7 @@ def test_fp32_indentation_tracks_oracle(tile):
     f_ref = np.hypot(hist[:, 0], hist[:, 1])
     f_got = np.hypot(fh[:, 0], fh[:, 1])
     peak = abs(f_got.max() - f_ref.max()) / f_ref.max()
-    print("fp32 indentation", tile, e, "peak force", peak, "redo", m.gpu.fp64_redo_count())
+    print(im.FORM_NAMES[form], "indentation", tile, e, "peak force", peak, "redo", m.gpu.fp64_redo_count())
     assert f_ref.max() > 0
     assert e["disp_h"] < 1e-3 and e["vel"] < 1e-2 and e["strain"] < 1e-2, e
     assert peak < 1e-2
