@@ -389,10 +389,15 @@ static int scan_ints(icm_ctx *c, const int *in, int n, int *chunk, int *out)
         ICM_CUDA(cudaMemsetAsync(out, 0, sizeof(int), c->stream));
         return ICM_OK;
     }
+    // a few chunks: one block; more: the chunks' sums, then each chunk's
+    // scan offset by the sums before it
+    if (n <= kScanThreads * kScanSmallItems) {
+        k_scan_small<<<1, kScanThreads, 0, c->stream>>>(in, n, out);
+        ICM_LAUNCHED("k_scan_small");
+        return ICM_OK;
+    }
     k_scan_chunks<<<nchunks, kScanThreads, 0, c->stream>>>(in, n, chunk);
     ICM_LAUNCHED("k_scan_chunks");
-    k_scan_sums<<<1, kScanThreads, 0, c->stream>>>(chunk, nchunks);
-    ICM_LAUNCHED("k_scan_sums");
     k_scan_apply<<<nchunks, kScanThreads, 0, c->stream>>>(in, n, chunk, out);
     ICM_LAUNCHED("k_scan_apply");
     return ICM_OK;
@@ -429,14 +434,10 @@ static int pack(icm_ctx *c, const icy_SimParams &P)
     k_bin_order<<<(int)((ncells + 255) / 256), 256, 0, s>>>((int)ncells, c->bin.cell_start, c->bin.perm);
     ICM_LAUNCHED("k_bin_order");
     ICM_CUDA(cudaMemsetAsync(c->bin.nbusy, 0, sizeof(int), s));
-    k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start,
-                                                          c->bin.nbusy);
-    ICM_LAUNCHED("k_tile_starts");
-    k_lane_order<<<ntiles, 256, 0, s>>>(g.TX * g.TY, c->bin.cell_start, c->bin.lane_cell, c->bin.cell_lane);
+    k_lane_order<<<(ntiles + kLaneOrderWarps - 1) / kLaneOrderWarps, 32 * kLaneOrderWarps, 0, s>>>(
+        ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.lane_cell, c->bin.cell_lane, c->bin.group_slots,
+        c->bin.tile_start, c->bin.nbusy);
     ICM_LAUNCHED("k_lane_order");
-    k_group_slots<<<(ngroups + 255) / 256, 256, 0, s>>>(ngroups, c->bin.cell_start, c->bin.lane_cell,
-                                                        c->bin.group_slots);
-    ICM_LAUNCHED("k_group_slots");
     if ((rc = scan_ints(c, c->bin.group_slots, ngroups, c->bin.gchunk, c->bin.group_base))) return rc;
     int nslots = 0, nbusy = 0;
     ICM_CUDA(cudaMemcpyAsync(&nslots, c->bin.group_base + ngroups, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -622,14 +623,10 @@ static int rebin_begin(icm_ctx *c, const icy_SimParams &P)
     k_rebin_order<<<(int)((ncells + 255) / 256), 256, 0, s>>>((int)ncells, c->bin.cell_start, c->bin.perm, c->bin.pid);
     ICM_LAUNCHED("k_rebin_order");
     ICM_CUDA(cudaMemsetAsync(c->bin.nbusy, 0, sizeof(int), s));
-    k_tile_starts<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.tile_start,
-                                                          c->bin.nbusy);
-    ICM_LAUNCHED("k_tile_starts");
-    k_lane_order<<<ntiles, 256, 0, s>>>(g.TX * g.TY, c->bin.cell_start, c->bin.lane_cell, c->bin.cell_lane);
+    k_lane_order<<<(ntiles + kLaneOrderWarps - 1) / kLaneOrderWarps, 32 * kLaneOrderWarps, 0, s>>>(
+        ntiles, g.TX * g.TY, c->bin.cell_start, c->bin.lane_cell, c->bin.cell_lane, c->bin.group_slots,
+        c->bin.tile_start, c->bin.nbusy);
     ICM_LAUNCHED("k_lane_order");
-    k_group_slots<<<(ngroups + 255) / 256, 256, 0, s>>>(ngroups, c->bin.cell_start, c->bin.lane_cell,
-                                                        c->bin.group_slots);
-    ICM_LAUNCHED("k_group_slots");
     if ((rc = scan_ints(c, c->bin.group_slots, ngroups, c->bin.gchunk, c->bin.group_base))) return rc;
     if (!c->h_ns && cudaMallocHost((void **)&c->h_ns, 2 * sizeof(int)) != cudaSuccess) {
         c->h_ns = nullptr;
@@ -775,7 +772,13 @@ static int tile_order(icm_ctx *c, int ntiles, const int *&order, int &nlaunch)
     }
     if (ntiles > kMaxOrderTiles) return ICM_OK;
     const int max_split = std::min(std::max(c->split_max, 0), ntiles);
-    k_tile_order<<<1, kOrderThreads, sizeof(int) * (size_t)ntiles, c->stream>>>(
+    static bool opted = false;  // 2 ints per tile: above 48 KB from 6,144 tiles
+    if (!opted) {
+        ICM_CUDA(cudaFuncSetAttribute(k_tile_order, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(2 * sizeof(int) * kMaxOrderTiles)));
+        opted = true;
+    }
+    k_tile_order<<<1, kOrderThreads, 2 * sizeof(int) * (size_t)ntiles, c->stream>>>(
         ntiles, c->fz.cost, c->bin.tile_start, max_split, (float)c->split_ratio, c->fz.order, c->fz.empties);
     ICM_LAUNCHED("k_tile_order");
     c->pdl_next = false;  // the substep reads the order before its dependency wait

@@ -1813,18 +1813,22 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *tmp, int &total)
 // cost exceeds ratio times the mean over tiles holding particles, at most
 // max_split: their two halves lead the order (two CTAs each). The order has
 // n + max_split entries, the unused ones -1; a launch needs its first
-// busy + S + ceil((n - busy) / kEmptyPerCta). Dynamic shared memory: n ints.
+// busy + S + ceil((n - busy) / kEmptyPerCta). Dynamic shared memory: 2 n ints.
 constexpr int kOrderLevels = kOrderThreads;
 
 __global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsigned *cost, const int *tile_start,
                                                               int max_split, float ratio, int *order, int *empties)
 {
     extern __shared__ int s_sorted[];
+    // per tile: its cost (kNoCost: no particles), then its level
+    unsigned *s_c = reinterpret_cast<unsigned *>(s_sorted + n);
+    constexpr unsigned kNoCost = 0xffffffffu;
     __shared__ int s_off[kOrderLevels];
     __shared__ int s_tmp[32];
     __shared__ unsigned long long s_sum;
     __shared__ unsigned s_max;
     __shared__ int s_busy, s_over;
+    const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x;
     for (int b = tid; b < kOrderLevels; b += blockDim.x) s_off[b] = 0;
     if (tid == 0) {
@@ -1833,40 +1837,58 @@ __global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsig
         s_busy = 0;
         s_over = 0;
     }
-    __syncthreads();
-    auto busy_tile = [&](int i) { return tile_start[i + 1] > tile_start[i]; };
-    auto tile_cost = [&](int i) -> unsigned {
-        const unsigned long long cc = (unsigned long long)cost[i] + cost[n + i];
-        return cc > 0xffffffffull ? 0xffffffffu : (unsigned)cc;
-    };
     unsigned long long sum = 0;
     unsigned mx = 0;
     int busy = 0;
-    for (int i = tid; i < n; i += blockDim.x)
-        if (busy_tile(i)) {
-            const unsigned c = tile_cost(i);
+    for (int i = tid; i < n; i += blockDim.x) {
+        unsigned c = kNoCost;
+        if (tile_start[i + 1] > tile_start[i]) {
+            const unsigned long long cc = (unsigned long long)cost[i] + cost[n + i];
+            c = cc >= kNoCost ? kNoCost - 1 : (unsigned)cc;
             sum += c;
             busy++;
             mx = max(mx, c);
         }
-    atomicAdd(&s_sum, sum);
-    atomicAdd(&s_busy, busy);
-    atomicMax(&s_max, mx);
+        s_c[i] = c;
+    }
+    // one shared atomic per warp (a thousand on one address serialise, the
+    // 64-bit sum as a compare-and-swap loop)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(FULL, sum, o);
+    busy = __reduce_add_sync(FULL, busy);
+    mx = __reduce_max_sync(FULL, mx);
+    __syncthreads();  // s_off and the totals are zero
+    if ((tid & 31) == 0) {
+        atomicAdd(&s_sum, sum);
+        atomicAdd(&s_busy, busy);
+        atomicMax(&s_max, mx);
+    }
     __syncthreads();
     const unsigned cmax = max(s_max, 1u);
     const int nbusy = s_busy;
-    // busy tiles take levels 1 .. kOrderLevels - 1 (the heaviest the top
-    // one), tiles without particles level 0
-    auto level = [&](int i) -> int {
-        return busy_tile(i) ? 1 + (int)((unsigned long long)tile_cost(i) * (kOrderLevels - 2) / cmax) : 0;
-    };
     const double thr = nbusy > 0 ? (double)ratio * (double)s_sum / (double)nbusy : 1e300;
+    // busy tiles take levels 1 .. kOrderLevels - 1 (the heaviest the top
+    // one), tiles without particles level 0. Most tiles hold no particles
+    // and share level 0: a warp adds once per distinct level (shared atomics
+    // on one address serialise).
     int over = 0;
-    for (int i = tid; i < n; i += blockDim.x) {
-        atomicAdd(&s_off[level(i)], 1);
-        over += busy_tile(i) && (double)tile_cost(i) > thr;
+    for (int i0 = tid - (tid & 31); i0 < n; i0 += blockDim.x) {
+        const int i = i0 + (tid & 31);
+        int lv = -1;
+        if (i < n) {
+            const unsigned c = s_c[i];
+            lv = 0;
+            if (c != kNoCost) {
+                lv = 1 + (int)((unsigned long long)c * (kOrderLevels - 2) / cmax);
+                over += (double)c > thr;
+            }
+            s_c[i] = (unsigned)lv;
+        }
+        const unsigned peers = __match_any_sync(FULL, lv);
+        if (lv >= 0 && (tid & 31) == __ffs(peers) - 1) atomicAdd(&s_off[lv], __popc(peers));
     }
-    atomicAdd(&s_over, over);
+    over = __reduce_add_sync(FULL, over);
+    if ((tid & 31) == 0) atomicAdd(&s_over, over);
     __syncthreads();
     // start of each level in descending level order: thread t takes level
     // kOrderLevels - 1 - t (blockDim.x == kOrderLevels)
@@ -1878,7 +1900,17 @@ __global__ void __launch_bounds__(kOrderThreads) k_tile_order(int n, const unsig
         s_off[b] = before;
     }
     __syncthreads();
-    for (int i = tid; i < n; i += blockDim.x) s_sorted[atomicAdd(&s_off[level(i)], 1)] = i;
+    for (int i0 = tid - (tid & 31); i0 < n; i0 += blockDim.x) {
+        const int i = i0 + (tid & 31);
+        const int lv = i < n ? (int)s_c[i] : -1;
+        const unsigned peers = __match_any_sync(FULL, lv);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (lv >= 0 && (tid & 31) == leader) base = atomicAdd(&s_off[lv], __popc(peers));
+        base = __shfl_sync(FULL, base, leader);
+        // places in lane order within the warp's share of the level
+        if (lv >= 0) s_sorted[base + __popc(peers & ((1u << (tid & 31)) - 1))] = i;
+    }
     __syncthreads();
     const int S = min(min(s_over, max_split), nbusy);
     const int nempty = n - nbusy, ngroups = (nempty + kEmptyPerCta - 1) / kEmptyPerCta;
@@ -1909,29 +1941,54 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_chunks(const int *in, int
     if (threadIdx.x == 0) chunk_sums[blockIdx.x] = total;
 }
 
-// single block: exclusive scan of up to kScanChunk chunk sums in place
-__global__ void __launch_bounds__(kScanThreads) k_scan_sums(int *sums, int n)
+// One block: exclusive scan of a short array (n <= kScanThreads *
+// kScanSmallItems), and out[n] = the total. Warp w takes a run of seg
+// consecutive entries (seg a multiple of 32) and reads it in rows of 32
+// (coalesced): once to add it up, and after the block has scanned the warps'
+// sums, again to scan it row by row with warp shuffles.
+constexpr int kScanSmallItems = 32;
+__global__ void __launch_bounds__(kScanThreads) k_scan_small(const int *in, int n, int *out)
 {
     __shared__ int tmp[32];
-    int base = threadIdx.x * kScanItems;
-    int v[kScanItems], s = 0;
-#pragma unroll
-    for (int k = 0; k < kScanItems; k++) {
-        v[k] = (base + k < n) ? sums[base + k] : 0;
-        s += v[k];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int seg = (n + 32 * nw - 1) / (32 * nw) * 32;
+    const int e0 = w * seg;
+    int s = 0;
+    for (int r = 0; r < seg; r += 32) {
+        const int e = e0 + r + lane;
+        if (e < n) s += in[e];
     }
+    s = __reduce_add_sync(FULL, s);
     int total;
-    int before = block_exclusive_scan(s, tmp, total);
+    int off = block_exclusive_scan(lane == 0 ? s : 0, tmp, total);
+    off = __shfl_sync(FULL, off, 0);  // the sum of the warps before this one
+#pragma unroll 4
+    for (int r = 0; r < seg; r += 32) {
+        const int e = e0 + r + lane;
+        const int x = e < n ? in[e] : 0;
+        int y = x;
 #pragma unroll
-    for (int k = 0; k < kScanItems; k++) {
-        if (base + k < n) sums[base + k] = before;
-        before += v[k];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int z = __shfl_up_sync(FULL, y, o);
+            if (lane >= o) y += z;
+        }
+        if (e < n) out[e] = off + y - x;
+        off += __shfl_sync(FULL, y, 31);
     }
+    if (threadIdx.x == 0) out[n] = total;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int *in, int n, const int *chunk_off, int *out)
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int *in, int n, const int *chunk_sums, int *out)
 {
     __shared__ int tmp[32];
+    int off = 0;
+    for (int i = threadIdx.x; i < (int)blockIdx.x; i += blockDim.x) off += chunk_sums[i];
+    {
+        int total;
+        block_exclusive_scan(off, tmp, total);
+        off = total;
+    }
     int base = blockIdx.x * kScanChunk + threadIdx.x * kScanItems;
     int v[kScanItems], s = 0;
 #pragma unroll
@@ -1940,7 +1997,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int *in, int 
         s += v[k];
     }
     int total;
-    int before = block_exclusive_scan(s, tmp, total) + chunk_off[blockIdx.x];
+    int before = block_exclusive_scan(s, tmp, total) + off;
 #pragma unroll
     for (int k = 0; k < kScanItems; k++) {
         if (base + k < n) out[base + k] = before;
@@ -1971,64 +2028,79 @@ __global__ void k_bin_order(int ncells, const int *start, int *perm)
     }
 }
 
-// Lane order of the cells of each tile (one CTA per tile, cells_per_tile a
-// power of two <= kMaxTileCells): by particle count, fullest first, ties by
-// cell key. lane_cell[l] is the cell key at lane l and cell_lane its inverse;
-// both index the tile's own range of keys, t * cells_per_tile + i. A group
-// of 32 consecutive lanes then holds cells of similar counts, so that few of
-// its lanes idle through the rounds of its fullest cell.
-constexpr int kMaxTileCells = 512;
+// Lane order of the cells of each tile (one warp per tile, cells_per_tile a
+// multiple of 32 and at most kMaxTileCells): by particle count, fullest
+// first, ties by cell key. lane_cell[l] is the cell key at lane l and
+// cell_lane its inverse; both index the tile's own range of keys,
+// t * cells_per_tile + i. A group of 32 consecutive lanes then holds cells of
+// similar counts, so that few of its lanes idle through the rounds of its
+// fullest cell. The same pass writes what follows from the order:
+// group_slots (32 x the count of the group's first, fullest lane: its slots
+// in the ELL layout), tile_start[t] (the tile's first particle; the last
+// tile also writes tile_start[ntiles]) and *nbusy (tiles holding particles,
+// zeroed by the caller). The warp visits the distinct counts from the
+// largest down; at each it places the cells of that count in key order
+// (ballots over the tile's rows of 32 keys).
+constexpr int kMaxTileCells = 512, kLaneOrderWarps = 4;
 
-__global__ void __launch_bounds__(256) k_lane_order(int cells_per_tile, const int *cell_start, int *lane_cell,
-                                                    int *cell_lane)
+__global__ void __launch_bounds__(32 * kLaneOrderWarps) k_lane_order(int ntiles, int cells_per_tile,
+                                                                    const int *cell_start, int *lane_cell,
+                                                                    int *cell_lane, int *group_slots,
+                                                                    int *tile_start, int *nbusy)
 {
-    __shared__ uint32_t s_key[kMaxTileCells];
-    const int base = blockIdx.x * cells_per_tile, n = cells_per_tile;
-    if (cell_start[base + n] == cell_start[base]) {
+    constexpr int kRows = kMaxTileCells / 32;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int t = blockIdx.x * kLaneOrderWarps + (threadIdx.x >> 5);
+    if (t >= ntiles) return;
+    const int base = t * cells_per_tile, rows = cells_per_tile / 32;
+    const int first = cell_start[base], last = cell_start[base + cells_per_tile];
+    if (lane == 0) {
+        tile_start[t] = first;
+        if (t == ntiles - 1) tile_start[ntiles] = last;
+        if (last > first) atomicAdd(nbusy, 1);
+    }
+    if (last == first) {
         // no particles: every count is 0, and the order by key is the identity
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        for (int i = lane; i < cells_per_tile; i += 32) {
             lane_cell[base + i] = base + i;
             cell_lane[base + i] = base + i;
         }
+        if (lane < rows) group_slots[(base >> 5) + lane] = 0;
         return;
     }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int cnt = min(cell_start[base + i + 1] - cell_start[base + i], 0xffff);
-        s_key[i] = ((uint32_t)(0xffff - cnt) << 16) | (uint32_t)i;  // ascending key = descending count
-    }
-    __syncthreads();
-    for (int k = 2; k <= n; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const uint32_t a = s_key[i], b = s_key[l];
-                    if (((i & k) == 0) ? (a > b) : (a < b)) {
-                        s_key[i] = b;
-                        s_key[l] = a;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int cell = (int)(s_key[i] & 0xffffu);
-        lane_cell[base + i] = base + cell;
-        cell_lane[base + cell] = base + i;
-    }
-}
-
-// Slots of each group of 32 consecutive lanes: 32 x the largest count.
-__global__ void k_group_slots(int ngroups, const int *cell_start, const int *lane_cell, int *group_slots)
-{
-    int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ngroups) return;
+    int cnt[kRows];
     int mx = 0;
-    for (int l = 0; l < 32; l++) {
-        const int c = lane_cell[g * 32 + l];
-        mx = max(mx, cell_start[c + 1] - cell_start[c]);
+#pragma unroll
+    for (int r = 0; r < kRows; r++) {
+        cnt[r] = -1;
+        if (r < rows) {
+            const int i = base + 32 * r + lane;
+            cnt[r] = cell_start[i + 1] - cell_start[i];
+            mx = max(mx, cnt[r]);
+        }
     }
-    group_slots[g] = 32 * mx;
+    int v = __reduce_max_sync(FULL, mx);
+    int pos = 0;  // lanes placed so far
+    const unsigned below = (1u << lane) - 1u;
+    while (v >= 0) {
+        int next = -1;
+#pragma unroll
+        for (int r = 0; r < kRows; r++) {
+            if (r >= rows) break;
+            const bool mine = cnt[r] == v;
+            const unsigned b = __ballot_sync(FULL, mine);
+            if (mine) {
+                const int l = pos + __popc(b & below), cell = 32 * r + lane;
+                lane_cell[base + l] = base + cell;
+                cell_lane[base + cell] = base + l;
+                if ((l & 31) == 0) group_slots[(base + l) >> 5] = 32 * v;
+            }
+            pos += __popc(b);
+            if (cnt[r] < v) next = max(next, cnt[r]);
+        }
+        v = __reduce_max_sync(FULL, next);
+    }
 }
 
 // Slot of particle r of the cell with key k.
@@ -2044,15 +2116,6 @@ __device__ __forceinline__ int slot_of(int q, const int *perm, const int *key, c
 {
     const int k = key[perm[q]];
     return slot_in_cell(k, q - cell_start[k], cell_lane, group_base);
-}
-
-// tile_start[t] = first particle of tile t; *nbusy (zeroed by the caller)
-// counts the tiles holding particles
-__global__ void k_tile_starts(int ntiles, int cells_per_tile, const int *cell_start, int *tile_start, int *nbusy)
-{
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t <= ntiles) tile_start[t] = cell_start[t * cells_per_tile];
-    if (t < ntiles && cell_start[(t + 1) * cells_per_tile] > cell_start[t * cells_per_tile]) atomicAdd(nbusy, 1);
 }
 
 __device__ __forceinline__ uint32_t read_meta(const icy_SimParams &P, int i)
