@@ -102,7 +102,7 @@ struct icm_ctx {
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     int form = ICM_FORM_FP64_STEPWISE;
     int tile_variant = 1, threads = 128;
-    int rebin_interval = 200;
+    int rebin_interval = 100;
     // heavy tiles run as two CTAs: at most split_max tiles whose measured
     // cost exceeds split_ratio times the mean over tiles with particles
     int split_max = 128;

@@ -110,7 +110,7 @@ int icm_set_tile(icm_ctx *ctx, int tile_variant, int threads);
 int icm_get_tile(icm_ctx *ctx, int *tile_variant, int *threads);
 /* Fused forms: re-bin the particles by their current grid cell every
  * `substeps` substeps of a run of icm_run_substeps, counted from the run's
- * start and never after its last substep (default 200). 0: only when the
+ * start and never after its last substep (default 100). 0: only when the
  * particles are packed (the first run after an upload or a change of form
  * or tile). Particles that left their binned cell take a slower scatter
  * path until then. */
