@@ -46,6 +46,8 @@ HARVEST_CONFIG, HARVEST_EVERY, HARVEST_CAP = "c2_250k", 5, 4_000_000
 # cases of the ensemble workload, 3,000 substeps
 HARVEST_ENS_CASES, HARVEST_ENS_SUBSTEPS, HARVEST_ENS_CAP = 16, 3000, 1_000_000
 SUR_STEPS, SUR_TILES, SUR_TOL = 3000, 64, 0.02
+# re-binning interval of the ensemble and of its per-case arms
+ENS_REBIN = 200
 
 
 def parse():
@@ -740,6 +742,7 @@ def ensemble_section(args, device, flush):
         ms = [configs.c4_model(c, device) for c in cases]
         for m in ms:
             m.gpu.set_form(form)
+            m.gpu.set_rebin_interval(ENS_REBIN)  # as the ensemble arm
         return ms
 
     def close(ms):
@@ -808,6 +811,7 @@ def ensemble_section(args, device, flush):
     # covers the same substeps as the per-case arms
     models = fresh()
     ens = Ensemble(form, tile, threads, device=device)
+    ens.set(rebin_interval=ENS_REBIN)
     for m in models:
         ens.add(m)
     st = torch.cuda.ExternalStream(ens.stream_handle())
@@ -844,7 +848,7 @@ def ensemble_section(args, device, flush):
                       "speedup_vs_sequential": seq_ms / ens_ms, "speedup_vs_concurrent_streams": conc_ms / ens_ms},
         "tile": im.TILE_VARIANTS[tile], "threads": threads, "tile_choice": note,
         "timing": f"every arm: fresh copies of the same cases, {WARM} warm-up substeps (packing), then timed runs "
-                  f"of {S} substeps (re-binned every 200), L2 flushed before each. Ensemble: {runs} runs, segments "
+                  f"of {S} substeps (re-binned every {ENS_REBIN}), L2 flushed before each. Ensemble: {runs} runs, segments "
                   "replayed from CUDA graphs (the first captures inside the first run); per-case arms: the first "
                   "run, through run_substeps",
         "gpu_launches_per_substep": 1,
