@@ -497,6 +497,18 @@ static int ensure_hist(icm_ctx *c, int n)
 
 // ----------------------------------------------------- fused run dispatch
 
+// cudaFuncSetAttribute acts on the current device, so the largest dynamic
+// shared memory a kernel has been opted in to is kept per device.
+constexpr int kMaxDevices = 64;
+static bool need_opt_in(const size_t *opted, int device, size_t dyn)
+{
+    return device < 0 || device >= kMaxDevices || dyn > opted[device];
+}
+static void opted_in(size_t *opted, int device, size_t dyn)
+{
+    if (device >= 0 && device < kMaxDevices) opted[device] = dyn;
+}
+
 // Dynamic shared memory of the per-warp accumulation regions; above 48 KB
 // the kernel has to opt in once.
 template <class Pol, int TX, int TY, int MODE>
@@ -508,11 +520,11 @@ static int launch_one(icm_ctx *c, int ntiles, const icy_SimParams &P, const type
     if (TX * TY > 32 * kMaxGroupsPerWarp * nwarps || nwarps > kMaxWarps)
         return icm::fail(ICM_ERR_ARG, "tile too large for the block size (need threads >= TX*TY/4)");
     const size_t dyn = tile_dyn_bytes<Pol, MODE>(RN, nwarps);
-    static size_t opted = 0;  // static + dynamic shared memory above 48 KB needs the opt-in
-    if (dyn > opted) {  // also needed when static + dynamic exceed 48 KB
+    static size_t opted[kMaxDevices] = {};  // static + dynamic shared memory above 48 KB needs the opt-in
+    if (need_opt_in(opted, c->device, dyn)) {
         ICM_CUDA(cudaFuncSetAttribute(k_tile_substep<Pol, TX, TY, MODE>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        opted = dyn;
+        opted_in(opted, c->device, dyn);
     }
     // programmatic dependent launch: the next substep's CTAs are launched
     // while this one's last wave runs, and wait in the kernel (griddepcontrol)
@@ -772,11 +784,11 @@ static int tile_order(icm_ctx *c, int ntiles, const int *&order, int &nlaunch)
     }
     if (ntiles > kMaxOrderTiles) return ICM_OK;
     const int max_split = std::min(std::max(c->split_max, 0), ntiles);
-    static bool opted = false;  // 2 ints per tile: above 48 KB from 6,144 tiles
-    if (!opted) {
-        ICM_CUDA(cudaFuncSetAttribute(k_tile_order, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)(2 * sizeof(int) * kMaxOrderTiles)));
-        opted = true;
+    static size_t opted[kMaxDevices] = {};  // 2 ints per tile: above 48 KB from 6,144 tiles
+    const size_t order_smem = 2 * sizeof(int) * kMaxOrderTiles;
+    if (need_opt_in(opted, c->device, order_smem)) {
+        ICM_CUDA(cudaFuncSetAttribute(k_tile_order, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)order_smem));
+        opted_in(opted, c->device, order_smem);
     }
     k_tile_order<<<1, kOrderThreads, 2 * sizeof(int) * (size_t)ntiles, c->stream>>>(
         ntiles, c->fz.cost, c->bin.tile_start, max_split, (float)c->split_ratio, c->fz.order, c->fz.empties);
@@ -1372,11 +1384,11 @@ int ens_launch_one(icm_ensemble *e, int grid, const void *d_cases, const EnsLaun
     constexpr int RN = (TX + 4) * (TY + 4);
     const int nwarps = e->threads / 32;
     const size_t dyn = tile_dyn_bytes<Pol, MODE>(RN, nwarps);
-    static size_t opted = 0;
-    if (dyn > opted) {
+    static size_t opted[kMaxDevices] = {};
+    if (need_opt_in(opted, e->device, dyn)) {
         ICM_CUDA(cudaFuncSetAttribute(k_tile_substep_ens<Pol, TX, TY, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)dyn));
-        opted = dyn;
+        opted_in(opted, e->device, dyn);
     }
     if (grid < 1) return ICM_OK;
     // a programmatic dependent of the previous launch, as single runs are

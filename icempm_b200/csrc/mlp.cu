@@ -406,14 +406,18 @@ template <class T> struct DevBuf {
     }
 };
 
+// the opt-in is per device (cudaFuncSetAttribute acts on the current one)
 int set_tile_smem()
 {
-    static bool done = false;
-    if (done) return ICM_OK;
+    constexpr int kMaxDevices = 64;
+    static bool done[kMaxDevices] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return icm::fail(ICM_ERR_CUDA, "mlp: cudaGetDevice");
+    if (dev >= 0 && dev < kMaxDevices && done[dev]) return ICM_OK;
     if (cudaFuncSetAttribute(k_mlp_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem) != cudaSuccess ||
         cudaFuncSetAttribute(k_mlp_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem) != cudaSuccess)
         return icm::fail(ICM_ERR_CUDA, "mlp: shared-memory opt-in failed");
-    done = true;
+    if (dev >= 0 && dev < kMaxDevices) done[dev] = true;
     return ICM_OK;
 }
 
