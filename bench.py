@@ -45,7 +45,7 @@ HARVEST_CONFIG, HARVEST_EVERY, HARVEST_CAP = "c2_250k", 5, 4_000_000
 # more pairs, from cases with other materials and indenters: the first 16
 # cases of the ensemble workload, 3,000 substeps
 HARVEST_ENS_CASES, HARVEST_ENS_SUBSTEPS, HARVEST_ENS_CAP = 16, 3000, 1_000_000
-SUR_STEPS, SUR_TILES, SUR_TOL = 3000, 64, 0.02
+SUR_STEPS, SUR_TILES, SUR_TOL = 3000, 296, 0.02  # 296 tiles: two CTAs on each of 148 SMs
 # re-binning interval of the ensemble and of its per-case arms
 ENS_REBIN = 200
 

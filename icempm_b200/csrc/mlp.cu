@@ -36,16 +36,23 @@ struct MlpTcNet {
 };
 
 constexpr int kRows = 128;
-constexpr uint32_t kTmemCols = 512;
-// TMEM columns of the accumulators (32-aligned starts)
-constexpr int cZ1 = 0, cZ2 = 64, cZ3 = 128, cDH2 = 160, cDH1 = 224, cDW3T = 288, cDW2 = 320, cDW1 = 384;
+// TMEM columns of the accumulators (32-aligned starts). Accumulators share
+// columns where one is dead before the next is written: Z3 is read before
+// dH2 is formed, Z2 (read for gelu' in dH2's epilogue) before dH1, dH2
+// (read in that epilogue) before dW2, dW3^T before dW1; Z1 stays for
+// gelu' of the last step. 256 columns let two CTAs share an SM's 512.
+constexpr uint32_t kTmemCols = 256;
+constexpr int cZ1 = 0, cZ2 = 64, cDH1 = 64, cZ3 = 128, cDH2 = 128, cDW2 = 128, cDW3T = 192, cDW1 = 192;
 constexpr int kWaitPolls = 1 << 24;
 
-// shared-memory layout of k_mlp_tile (bytes)
+// shared-memory layout of k_mlp_tile (bytes). dZ3 takes X's tile (read
+// only by the first product) and dZ2^T takes H2^T's (last read by the
+// product for dW3^T, which completes before dZ2 is formed): 98 KB, two CTAs
+// per SM.
 constexpr int sW1 = 0, sW2 = sW1 + 2048, sW3 = sW2 + 8192, sW3T = sW3 + 2048, sW2T = sW3T + 2048,
               sX = sW2T + 8192, sXT = sX + 4096, sH1 = sXT + 4096, sH1T = sH1 + 16384, sH2 = sH1T + 16384,
-              sH2T = sH2 + 16384, sDZ3 = sH2T + 16384, sDZ3T = sDZ3 + 4096, sDZ2T = sDZ3T + 4096,
-              kTileSmem = sDZ2T + 16384;
+              sH2T = sH2 + 16384, sDZ3T = sH2T + 16384, kTileSmem = sDZ3T + 4096;
+constexpr int sDZ3 = sX, sDZ2T = sH2T;
 
 __device__ __forceinline__ void put_bf16(unsigned char *base, int row, int k, int K, float v)
 {
@@ -80,6 +87,7 @@ struct TileArgs {
     const MlpTcNet *tc;      // BF16 operand tiles
     const float *net;        // FP32 parameters (biases, normalisation)
     float *grad;             // FP32 gradient (same layout as net), accumulated
+    size_t grad_stride;      // CTA b adds into grad + b * grad_stride (0: all into one)
     float *loss;             // accumulated mean squared error
     float *Yout;             // inference: denormalised outputs [n][3]
     int *status;             // set to 1 when a wait gives up
@@ -93,6 +101,10 @@ __global__ void __launch_bounds__(kRows) k_mlp_tile(const TileArgs a)
     __shared__ uint32_t s_tmem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const float *net = a.net;
+    // this CTA's gradient: its own slice in training, so that the CTAs of a
+    // step do not contend for the same addresses (the Adam step adds the
+    // slices up)
+    float *grad = a.grad + (size_t)blockIdx.x * a.grad_stride;
 
     // sample of this row
     int idx;
@@ -217,7 +229,7 @@ __global__ void __launch_bounds__(kRows) k_mlp_tile(const TileArgs a)
 #pragma unroll
         for (int o = 0; o < kMlpOut; o++) {
             const float s = warp_sum(dy[o]);
-            if (lane == 0) atomicAdd(&a.grad[kOffB3 + o], s);
+            if (lane == 0) atomicAdd(&grad[kOffB3 + o], s);
         }
         publish();
         // ---- dH2 = dZ3 W3 ; dW3^T = H2^T dZ3
@@ -240,13 +252,13 @@ __global__ void __launch_bounds__(kRows) k_mlp_tile(const TileArgs a)
                 put_bf16(sm + sH2, tid, c0 + j, 64, d);  // dZ2 over H2 (no longer read)
                 put_bf16(sm + sDZ2T, c0 + j, tid, kRows, d);
                 const float s = warp_sum(d);
-                if (lane == 0) atomicAdd(&a.grad[kOffB2 + c0 + j], s);
+                if (lane == 0) atomicAdd(&grad[kOffB2 + c0 + j], s);
             }
         }
         // dW3^T rows (hidden unit 16 warp + lane for lanes < 16)
         tc05::ld16(tc05::taddr(tmem, warp, cDW3T), dh);
         if (lane < 16)
-            for (int o = 0; o < kMlpOut; o++) atomicAdd(&a.grad[kOffW3 + o * kMlpHid + warp * 16 + lane], dh[o]);
+            for (int o = 0; o < kMlpOut; o++) atomicAdd(&grad[kOffW3 + o * kMlpHid + warp * 16 + lane], dh[o]);
         publish();
         // ---- dH1 = dZ2 W2 ; dW2 = dZ2^T H1
         if (tid == 0) {
@@ -268,14 +280,14 @@ __global__ void __launch_bounds__(kRows) k_mlp_tile(const TileArgs a)
                 const float d = dh[j] * gelu_grad(z[j] + net[kOffB1 + c0 + j]);
                 put_bf16(sm + sH1, c0 + j, tid, kRows, d);  // dZ1^T over H1 (no longer read)
                 const float s = warp_sum(d);
-                if (lane == 0) atomicAdd(&a.grad[kOffB1 + c0 + j], s);
+                if (lane == 0) atomicAdd(&grad[kOffB1 + c0 + j], s);
             }
         }
 #pragma unroll 1
         for (int c0 = 0; c0 < 64; c0 += 16) {
             tc05::ld16(tc05::taddr(tmem, warp, cDW2 + c0), dh);
             if (lane < 16)
-                for (int j = 0; j < 16; j++) atomicAdd(&a.grad[kOffW2 + (warp * 16 + lane) * kMlpHid + c0 + j], dh[j]);
+                for (int j = 0; j < 16; j++) atomicAdd(&grad[kOffW2 + (warp * 16 + lane) * kMlpHid + c0 + j], dh[j]);
         }
         publish();
         // ---- dW1 = dZ1^T X
@@ -288,7 +300,7 @@ __global__ void __launch_bounds__(kRows) k_mlp_tile(const TileArgs a)
         wait_mma();
         tc05::ld16(tc05::taddr(tmem, warp, cDW1), dh);
         if (lane < 16)
-            for (int i = 0; i < kMlpIn; i++) atomicAdd(&a.grad[kOffW1 + (warp * 16 + lane) * kMlpIn + i], dh[i]);
+            for (int i = 0; i < kMlpIn; i++) atomicAdd(&grad[kOffW1 + (warp * 16 + lane) * kMlpIn + i], dh[i]);
     }
     if (!ok && a.status) atomicExch(a.status, 1);
     tc05::fence_before_sync();
@@ -341,12 +353,14 @@ __global__ void k_mlp_prep(const float *net, MlpTcNet *tc, MlpWarpNet *wn)
 }
 
 // Adam on the weights and biases (not the normalisation)
-__global__ void k_mlp_adam(float *net, float *m, float *v, const float *grad, int count, float lr, float b1,
-                           float b2, float eps, float c1, float c2)
+// Adam step on the sum of nslices gradient slices (stride floats apart)
+__global__ void k_mlp_adam(float *net, float *m, float *v, const float *grad, int nslices, size_t stride, int count,
+                           float lr, float b1, float b2, float eps, float c1, float c2)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    const float g = grad[i];
+    float g = 0.f;
+    for (int b = 0; b < nslices; b++) g += grad[(size_t)b * stride + i];
     const float mi = b1 * m[i] + (1.f - b1) * g, vi = b2 * v[i] + (1.f - b2) * g * g;
     m[i] = mi;
     v[i] = vi;
@@ -515,7 +529,8 @@ extern "C" int icm_mlp_train(int device, const float *x, const float *y, int n, 
     DevBuf<int> status;
     const int steps = cfg->steps;
     if ((rc = X.alloc((size_t)n * kMlpIn)) || (rc = Y.alloc((size_t)n * kMlpOut)) || (rc = net.alloc(kMlpFloats)) ||
-        (rc = m.alloc(kMlpFloats)) || (rc = v.alloc(kMlpFloats)) || (rc = grad.alloc(kMlpFloats)) ||
+        (rc = m.alloc(kMlpFloats)) || (rc = v.alloc(kMlpFloats)) ||
+        (rc = grad.alloc((size_t)std::max(cfg->batch_tiles, 1) * kMlpFloats)) ||
         (rc = loss.alloc(std::max(steps, 1))) || (rc = tc.alloc(1)) || (rc = status.alloc(1)))
         return rc;
     cudaMemcpy(X.p, x, sizeof(float) * n * kMlpIn, cudaMemcpyHostToDevice);
@@ -536,11 +551,12 @@ extern "C" int icm_mlp_train(int device, const float *x, const float *y, int n, 
     a.tc = tc.p;
     a.net = net.p;
     a.grad = grad.p;
+    a.grad_stride = kMlpFloats;
     a.status = status.p;
     const int nw = kOffXMu;  // weights and biases
     for (int s = 0; s < steps; s++) {
         launch_prep(net.p, tc.p, nullptr);
-        cudaMemsetAsync(grad.p, 0, sizeof(float) * kMlpFloats);
+        cudaMemsetAsync(grad.p, 0, sizeof(float) * kMlpFloats * (size_t)cfg->batch_tiles);
         a.step = s;
         a.loss = loss.p + s;
         k_mlp_tile<true><<<cfg->batch_tiles, kRows, kTileSmem>>>(a);
@@ -548,7 +564,8 @@ extern "C" int icm_mlp_train(int device, const float *x, const float *y, int n, 
         const float frac = steps > 1 ? (float)s / (float)(steps - 1) : 0.f;
         const float lr = cfg->lr * (0.05f + 0.95f * 0.5f * (1.0f + std::cos(3.14159265f * frac)));
         const float c1 = 1.0f / (1.0f - std::pow(b1, (float)(s + 1))), c2 = 1.0f / (1.0f - std::pow(b2, (float)(s + 1)));
-        k_mlp_adam<<<(nw + 255) / 256, 256>>>(net.p, m.p, v.p, grad.p, nw, lr, b1, b2, eps, c1, c2);
+        k_mlp_adam<<<(nw + 255) / 256, 256>>>(net.p, m.p, v.p, grad.p, cfg->batch_tiles, kMlpFloats, nw, lr, b1, b2,
+                                              eps, c1, c2);
     }
     if ((rc = finish_device("icm_mlp_train", status.p))) return rc;
     cudaMemcpy(net_io, net.p, sizeof(float) * kMlpFloats, cudaMemcpyDeviceToHost);
