@@ -166,6 +166,27 @@ def test_ragged_grid_and_empty_tiles():
         assert e["crushed_mismatch"] == 0 and max(e["disp_rel"], e["vel"], e["strain"]) < FP64_TOL, (tile, e)
 
 
+@pytest.mark.parametrize("grid", [(1536, 1152), (2304, 1024)])
+def test_many_tiles(grid):
+    """Grids of 6,912 tiles of 16x16 cells (the tile sort's shared memory
+    above 48 KB) and of 9,216 tiles (beyond the sort's limit: launched in
+    tile order), re-binned every 3 substeps so that the sort runs on
+    measured costs, against the oracle."""
+    gx, gy = grid
+    p = params(gx, gy, dim=0.75 * gx / 96, dt=2e-6)
+    soa = scene(p, cells=(48, 12), seed=5, ind_y=0.05, perturb=2e-3, vel=0.05, crushed_frac=0.2)
+    q, ref, bins, err, hist = oracle_run(p, soa, 7)
+    for form in (im.FORM_FP64, im.FORM_FP32):
+        m = gpu_model(p, soa, form, 1, 128)
+        m.gpu.set_rebin_interval(3)
+        m.gpu.run_substeps(m.prms, 7)
+        e = compare_states(p, gpu_state(m), ref, soa)
+        tol = FP64_TOL if form == im.FORM_FP64 else 1e-3
+        assert m.gpu.error_code == 0 and max(e["disp_rel"], e["vel"], e["strain"]) < tol, (grid, form, e)
+        if form == im.FORM_FP64:
+            assert e["crushed_mismatch"] == 0, e
+
+
 def test_zero_particles():
     p = params(64, 32, dim=0.5, dt=2e-6)
     soa = scene(p, cells=(8, 4), seed=1)
