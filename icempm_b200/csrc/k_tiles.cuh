@@ -306,17 +306,23 @@ __device__ __forceinline__ bool tma_region_wait(uint64_t *bar, int *err)
 }
 
 struct Parts64 { double2 *pos; double4 *F; double *Jp; uint32_t *meta; double2 *vel; double4 *Bp; double2 *pq; };
-// FP32 form: X = {fraction x, fraction y, cell (pack_cell bits), meta word
-// (bits)}, one 16-byte vector, so that a particle's position and flags move
-// in one copy; H = Fe - I.
+// FP32 form: X = {fraction x, fraction y (32-bit fixed point, units of
+// 2^-32 cells), cell (pack_cell bits), meta word (bits)}, one 16-byte vector,
+// so that a particle's position and flags move in one copy; H = Fe - I;
+// Jp = Jp_inv - 1. Strain form for Jp_inv and fixed point for the position
+// keep the stored state as exact as the FP64 form's: a position fraction or
+// Jp_inv rounded to float each substep moves the 1M-particle indentation to
+// another outcome at 10,000 substeps (the crushing pattern bifurcates under
+// perturbations of 1e-8), while H rounded to float does not.
 struct Parts32 { float4 *X; float4 *H; float *Jp; float2 *vel; float4 *Bp; float2 *pq; };
 
 __host__ __device__ __forceinline__ uint32_t pack_cell(int ix, int iy) { return (uint32_t)(uint16_t)(int16_t)ix | ((uint32_t)(uint16_t)(int16_t)iy << 16); }
 __device__ __forceinline__ int cell_x(uint32_t c) { return (int)(int16_t)(uint16_t)(c & 0xffffu); }
 __device__ __forceinline__ int cell_y(uint32_t c) { return (int)(int16_t)(uint16_t)(c >> 16); }
-__device__ __forceinline__ float4 pack_x32(int ix, int iy, float fx, float fy, uint32_t meta)
+__device__ __forceinline__ float4 pack_x32(int ix, int iy, uint32_t ux, uint32_t uy, uint32_t meta)
 {
-    return make_float4(fx, fy, __uint_as_float(pack_cell(ix, iy)), __uint_as_float(meta));
+    return make_float4(__uint_as_float(ux), __uint_as_float(uy), __uint_as_float(pack_cell(ix, iy)),
+                       __uint_as_float(meta));
 }
 
 // Symmetric Kirchhoff stress as the P2G needs it.
@@ -442,7 +448,7 @@ struct Pol64 {
 // Appends a crushed particle's trial state (H, Jp_inv, meta word) to the
 // harvest buffer of the surrogate's training data (out of line: only
 // harvest substeps reach it).
-static __device__ __noinline__ void harvest_state(const Consts32 &k, const M2f H, const float Jp, const uint32_t meta)
+static __device__ __noinline__ void harvest_state(const Consts32 &k, const M2f H, const float jpm1, const uint32_t meta)
 {
     const unsigned slot = atomicAdd(k.harvest_n, 1u);
     if (slot >= k.harvest_cap) return;
@@ -451,7 +457,7 @@ static __device__ __noinline__ void harvest_state(const Consts32 &k, const M2f H
     h[1] = H.a01;
     h[2] = H.a10;
     h[3] = H.a11;
-    h[4] = Jp;
+    h[4] = 1.0f + jpm1;  // Jp_inv
     h[5] = __uint_as_float(meta);
 }
 
@@ -479,7 +485,9 @@ struct Pol32 {
     using Sums = CellSums<float>;
     using Consts = Consts32;
     using Tables = GrainTables32;
-    struct St { int ix, iy; float fx, fy; M2f H; float Jp; uint32_t meta; };
+    // position: cell (ix, iy) and fixed-point fraction (ux, uy) 2^-32; Jp:
+    // Jp_inv - 1
+    struct St { int ix, iy; uint32_t ux, uy; M2f H; float Jp; uint32_t meta; };
     struct Sten { int bx, by; float fx, fy, wx[3], wy[3]; };
     // one round of a warp (32 particles) staged in shared memory
     struct Stage { float4 H[32]; float4 X[32]; float Jp[32]; };
@@ -495,7 +503,7 @@ struct Pol32 {
         St s;
         const uint32_t c = __float_as_uint(X.z);
         s.ix = cell_x(c); s.iy = cell_y(c);
-        s.fx = X.x; s.fy = X.y;
+        s.ux = __float_as_uint(X.x); s.uy = __float_as_uint(X.y);
         s.H = {H.x, H.y, H.z, H.w};
         s.Jp = Jp;
         s.meta = __float_as_uint(X.w);
@@ -522,11 +530,13 @@ struct Pol32 {
             fr = X - (float)b;
         }
     }
+    // the fixed-point fraction as a float in [0, 1] (rounded only for use)
+    static __device__ __forceinline__ float frac(uint32_t u) { return __uint2float_rn(u) * 2.3283064365386963e-10f; }
     static __device__ __forceinline__ Sten stencil(const icy_SimParams &, const Consts &, const St &s)
     {
         Sten r;
-        base_of(s.ix, s.fx, r.bx, r.fx);
-        base_of(s.iy, s.fy, r.by, r.fy);
+        base_of(s.ix, frac(s.ux), r.bx, r.fx);
+        base_of(s.iy, frac(s.uy), r.by, r.fy);
         float a0 = 1.5f - r.fx, a1 = r.fx - 1.0f, a2 = r.fx - 0.5f;
         r.wx[0] = 0.5f * a0 * a0; r.wx[1] = 0.75f - a1 * a1; r.wx[2] = 0.5f * a2 * a2;
         float b0 = 1.5f - r.fy, b1 = r.fy - 1.0f, b2 = r.fy - 0.5f;
@@ -591,14 +601,14 @@ struct Pol32 {
     // position and H of the particle after a substep
     static __device__ __forceinline__ void advect(const Consts &k, St &s, float v0, float v1, const float B[4])
     {
-        // position: fraction inside the cell, renormalised to [0, 1)
-        float fx = s.fx + v0 * k.dt_h_inv, fy = s.fy + v1 * k.dt_h_inv;
-        float flx = floorf(fx), fly = floorf(fy);
-        s.ix += (int)flx; s.iy += (int)fly;
-        fx -= flx; fy -= fly;
-        if (fx >= 1.0f) { fx -= 1.0f; s.ix += 1; }
-        if (fy >= 1.0f) { fy -= 1.0f; s.iy += 1; }
-        s.fx = fx; s.fy = fy;
+        // position: the displacement in cells, to 2^-32 cells, added to the
+        // fixed-point fraction; carries move the cell
+        const long long x = (long long)s.ux + __float2ll_rn(v0 * k.dt_h_inv * 4294967296.0f);
+        const long long y = (long long)s.uy + __float2ll_rn(v1 * k.dt_h_inv * 4294967296.0f);
+        s.ix += (int)(x >> 32);
+        s.iy += (int)(y >> 32);
+        s.ux = (uint32_t)x;
+        s.uy = (uint32_t)y;
         // H_new = H + dt (C + C H)
         float c00 = k.dt * B[0], c01 = k.dt * B[1], c10 = k.dt * B[2], c11 = k.dt * B[3];
         M2f H = s.H;
@@ -612,7 +622,7 @@ struct Pol32 {
     {
         const Via64 o = constitutive32_via64(P, s.H, s.Jp, s.meta);
         s.H = o.H;
-        s.Jp = o.Jp;
+        s.Jp = o.jpm1;
         s.meta = o.meta;
         p_tr = o.p_tr;
         q_tr = o.q_tr;
@@ -640,7 +650,7 @@ struct Pol32 {
     }
     static __device__ __forceinline__ void store(const Parts &A, int p, const St &s, float jp_old, uint32_t)
     {
-        A.X[p] = pack_x32(s.ix, s.iy, s.fx, s.fy, s.meta);
+        A.X[p] = pack_x32(s.ix, s.iy, s.ux, s.uy, s.meta);
         A.H[p] = make_float4(s.H.a00, s.H.a01, s.H.a10, s.H.a11);
         if (s.Jp != jp_old) A.Jp[p] = s.Jp;
     }
@@ -652,7 +662,7 @@ struct Pol32 {
 
 // out-of-line steps of the surrogate form (a crushed particle is rare; the
 // hot loop keeps only the deferred state)
-struct SurrogateOut { M2f H; float Jp, p_tr, q_tr; int accepted, fp64; };
+struct SurrogateOut { M2f H; float jpm1, p_tr, q_tr; int accepted, fp64; };
 
 // The principal stretches s_i - 1 of a trial state from its FP32 invariants:
 // s_i^2 - 1 = e_i = me +- rho, s_i - 1 = e_i / (sqrt(1 + e_i) + 1).
@@ -666,13 +676,13 @@ __device__ __forceinline__ void stretches32(const Inv32 &v, float rho, float &s0
 // the network's input row (normalised features) of a crushed particle from
 // the FP32 invariants of its trial state; false (nothing written) when
 // det F <= 0.25, which the FP64 form takes
-static __device__ __noinline__ bool surrogate_defer(const Consts32 &k, __nv_bfloat16 *row, const M2f H, const float Jp)
+static __device__ __noinline__ bool surrogate_defer(const Consts32 &k, __nv_bfloat16 *row, const M2f H, const float jpm1)
 {
     const Inv32 v = invariants32(H, k.mu, k.kappa);
     if (!(v.J > 0.25f)) return false;
     float s0m1, s1m1;
     stretches32(v, sqrtf(v.hd * v.hd + v.b01 * v.b01), s0m1, s1m1);
-    const float x[kMlpIn] = {1e3f * s0m1, 1e3f * s1m1, 1e2f * (Jp - 1.0f), k.kappa * 1e-9f, k.tan_phi,
+    const float x[kMlpIn] = {1e3f * s0m1, 1e3f * s1m1, 1e2f * jpm1, k.kappa * 1e-9f, k.tan_phi,
                              k.dp_qmax * 1e-7f};
 #pragma unroll
     for (int j = 0; j < 8; j++) row[j] = __float2bfloat16(j < kMlpIn ? (x[j] - k.mlp->x_mu[j]) * k.mlp->x_isd[j] : 0.f);
@@ -684,7 +694,7 @@ static __device__ __noinline__ bool surrogate_defer(const Consts32 &k, __nv_bflo
 // its discontinuities); all in FP32 strain form from the trial state's
 // invariants, recomputed here rather than carried through the round
 static __device__ __noinline__ SurrogateOut surrogate_finish(const icy_SimParams &P, const Consts32 &k, const float *y,
-                                                             const M2f H, const float Jp, const uint32_t meta)
+                                                             const M2f H, const float jpm1, const uint32_t meta)
 {
     const Inv32 v = invariants32(H, k.mu, k.kappa);
     const float rho = sqrtf(v.hd * v.hd + v.b01 * v.b01);
@@ -696,9 +706,9 @@ static __device__ __noinline__ SurrogateOut surrogate_finish(const icy_SimParams
     const float ds0 = 1e-3f * (y[0] * k.mlp->y_sd[0] + k.mlp->y_mu[0]);
     const float ds1 = 1e-3f * (y[1] * k.mlp->y_sd[1] + k.mlp->y_mu[1]);
     const float tol = k.mlp_tol;
-    SurrogateOut o{H, Jp, p, q, 0, 0};
+    SurrogateOut o{H, jpm1, p, q, 0, 0};
     bool ok = false, moved = false;
-    if (!(p < -k.p_thr || Jp < 1.0f) && isfinite(ds0) && isfinite(ds1) && s0 + ds0 > 0.0f && s1 + ds1 > 0.0f) {
+    if (!(p < -k.p_thr || jpm1 < 0.0f) && isfinite(ds0) && isfinite(ds1) && s0 + ds0 > 0.0f && s1 + ds1 > 0.0f) {
         const float qn = (p > k.dp_pmax) ? 0.0f : fminf((p + k.p_thr) * k.tan_phi, k.dp_qmax);
         if (q >= qn) {
             // q of the predicted stretches: mu/(s0' s1') (s0' - s1')(s0' + s1')
@@ -717,10 +727,10 @@ static __device__ __noinline__ SurrogateOut surrogate_finish(const icy_SimParams
         o.accepted = 1;
         return o;
     }
-    if (!(v.J > 0.25f) || dp_map32(k, o.H, o.Jp, v, p, q, rho) != kC32_OK) {
-        const Via64 r = constitutive32_via64(P, H, Jp, meta);
+    if (!(v.J > 0.25f) || dp_map32(k, o.H, o.jpm1, v, p, q, rho) != kC32_OK) {
+        const Via64 r = constitutive32_via64(P, H, jpm1, meta);
         o.H = r.H;
-        o.Jp = r.Jp;
+        o.jpm1 = r.jpm1;
         o.p_tr = r.p_tr;
         o.q_tr = r.q_tr;
         o.fp64 = 1;
@@ -751,7 +761,7 @@ struct Pol32S : Pol32 {
     // shared memory, not registers, so the round's register use is the FP32
     // form's; with the network's rows the extra is 9 KB per CTA, which
     // keeps four 128-thread CTAs per SM.
-    struct Held { int p; uint32_t cell; float fx, fy, H[4], v0, v1, B[4]; };
+    struct Held { int p; uint32_t cell, ux, uy; float H[4], v0, v1, B[4]; };
     struct Tables : GrainTables32 {
         alignas(16) unsigned char rows[kWarps][32 * 16];  // network input/output rows, one per lane
         Held held[kWarps][32];
@@ -759,7 +769,7 @@ struct Pol32S : Pol32 {
     static __device__ __forceinline__ void defer_save(Tables &T, int p, const St &s, float v0, float v1,
                                                       const float B[4], float, uint32_t)
     {
-        T.held[threadIdx.x >> 5][threadIdx.x & 31] = {p, pack_cell(s.ix, s.iy), s.fx, s.fy,
+        T.held[threadIdx.x >> 5][threadIdx.x & 31] = {p, pack_cell(s.ix, s.iy), s.ux, s.uy,
                                                       {s.H.a00, s.H.a01, s.H.a10, s.H.a11}, v0, v1,
                                                       {B[0], B[1], B[2], B[3]}};
     }
@@ -770,8 +780,8 @@ struct Pol32S : Pol32 {
         p = h.p;
         s.ix = cell_x(h.cell);
         s.iy = cell_y(h.cell);
-        s.fx = h.fx;
-        s.fy = h.fy;
+        s.ux = h.ux;
+        s.uy = h.uy;
         s.H = {h.H[0], h.H[1], h.H[2], h.H[3]};
         s.Jp = A.Jp[p];
         s.meta = __float_as_uint(A.X[p].w);
@@ -817,7 +827,7 @@ struct Pol32S : Pol32 {
             surrogate_finish(P, k, reinterpret_cast<const float *>(T.rows[threadIdx.x >> 5] + (threadIdx.x & 31) * 16),
                              s.H, s.Jp, s.meta);
         s.H = o.H;
-        s.Jp = o.Jp;
+        s.Jp = o.jpm1;
         p_tr = o.p_tr;
         q_tr = o.q_tr;
         accepted += o.accepted;
@@ -2179,20 +2189,22 @@ __global__ void k_pack32(const icy_SimParams P, const int *perm, const int *key,
     const size_t pp = P.nPtsPitch;
     auto row = [&](int r) { return pts[(size_t)r * pp + i]; };
     pid[k] = i;
-    double X = row(ICM_IDX_POSX) * P.cellsize_inv, Y = row(ICM_IDX_POSX + 1) * P.cellsize_inv;
-    double fx = floor(X), fy = floor(Y);
-    float rx = (float)(X - fx), ry = (float)(Y - fy);
+    // cell and 32-bit fixed-point fraction of the position (a fraction that
+    // rounds up to a whole cell carries into the cell)
+    const double X = row(ICM_IDX_POSX) * P.cellsize_inv, Y = row(ICM_IDX_POSX + 1) * P.cellsize_inv;
+    const double fx = floor(X), fy = floor(Y);
+    long long ux = llrint((X - fx) * 4294967296.0), uy = llrint((Y - fy) * 4294967296.0);
     int ix = (int)fx, iy = (int)fy;
-    if (rx >= 1.0f) { rx = 0.0f; ix += 1; }
-    if (ry >= 1.0f) { ry = 0.0f; iy += 1; }
+    if (ux >= 4294967296ll) { ux -= 4294967296ll; ix += 1; }
+    if (uy >= 4294967296ll) { uy -= 4294967296ll; iy += 1; }
     const int16_t *gr = (const int16_t *)((const char *)P.pts_array + P.nPtsPitch);
-    A.X[k] = pack_x32(ix, iy, rx, ry, grain_meta32(gr[i], ((const uint8_t *)P.pts_array)[i]));
+    A.X[k] = pack_x32(ix, iy, (uint32_t)ux, (uint32_t)uy, grain_meta32(gr[i], ((const uint8_t *)P.pts_array)[i]));
     A.vel[k] = make_float2((float)row(ICM_IDX_VELX), (float)row(ICM_IDX_VELX + 1));
     A.H[k] = make_float4((float)(row(ICM_IDX_FE00) - 1.0), (float)row(ICM_IDX_FE00 + 1), (float)row(ICM_IDX_FE00 + 2),
                          (float)(row(ICM_IDX_FE00 + 3) - 1.0));
     A.Bp[k] = make_float4((float)row(ICM_IDX_BP00), (float)row(ICM_IDX_BP00 + 1), (float)row(ICM_IDX_BP00 + 2),
                           (float)row(ICM_IDX_BP00 + 3));
-    A.Jp[k] = (float)row(ICM_IDX_JP_INV);
+    A.Jp[k] = (float)(row(ICM_IDX_JP_INV) - 1.0);  // strain form
 }
 
 __global__ void k_unpack32(const icy_SimParams P, int nslots, const int *pid, const Parts32 A, int write_pq)
@@ -2206,15 +2218,15 @@ __global__ void k_unpack32(const icy_SimParams P, int nslots, const int *pid, co
     auto row = [&](int r) -> double & { return pts[(size_t)r * pp + i]; };
     const float4 X = A.X[k];
     const uint32_t c = __float_as_uint(X.z);
-    const float2 f = make_float2(X.x, X.y), v = A.vel[k];
+    const float2 v = A.vel[k];
     float4 H = A.H[k], B = A.Bp[k];
-    row(ICM_IDX_POSX) = ((double)cell_x(c) + (double)f.x) * P.cellsize;
-    row(ICM_IDX_POSX + 1) = ((double)cell_y(c) + (double)f.y) * P.cellsize;
+    row(ICM_IDX_POSX) = ((double)cell_x(c) + (double)__float_as_uint(X.x) * 0x1p-32) * P.cellsize;
+    row(ICM_IDX_POSX + 1) = ((double)cell_y(c) + (double)__float_as_uint(X.y) * 0x1p-32) * P.cellsize;
     row(ICM_IDX_VELX) = v.x; row(ICM_IDX_VELX + 1) = v.y;
     row(ICM_IDX_FE00) = 1.0 + (double)H.x; row(ICM_IDX_FE00 + 1) = H.y;
     row(ICM_IDX_FE00 + 2) = H.z; row(ICM_IDX_FE00 + 3) = 1.0 + (double)H.w;
     row(ICM_IDX_BP00) = B.x; row(ICM_IDX_BP00 + 1) = B.y; row(ICM_IDX_BP00 + 2) = B.z; row(ICM_IDX_BP00 + 3) = B.w;
-    row(ICM_IDX_JP_INV) = A.Jp[k];
+    row(ICM_IDX_JP_INV) = 1.0 + (double)A.Jp[k];
     ((uint8_t *)pts)[i] = (uint8_t)meta32_crushed(__float_as_uint(X.w));
     if (write_pq) {
         float2 q = A.pq[k];

@@ -175,7 +175,10 @@ constexpr float kDpMargin = 1e-4f;
 // accuracy:
 // * hydrostatic branch (p < -p_thr or Jp_inv < 1): s_new_i^2 = Je_new, so
 //   r_i^2 - 1 = (Je_new - 1 - e_i)/(1 + e_i) with e_i = me +- rho, and
-//   Jp_inv *= Je_new / J;
+//   Jp_inv *= Je_new / J, in strain form as the state keeps it (jpm1 =
+//   Jp_inv - 1): with f - 1 = (Je_new - 1 - (J - 1)) / J, jpm1 += (f - 1) +
+//   jpm1 (f - 1). (The factor rounded to float, 6e-8, moves the 1M-particle
+//   indentation to another outcome at 10,000 substeps; see the design notes.)
 // * cone (q >= q_n+1): the mean of s^2 is kept and its half-gap rho becomes
 //   rho q_n+1 / q, so e_new_i - e_i = +-(rho_new - rho) and
 //   r_i^2 - 1 = (e_new_i - e_i)/(1 + e_i);
@@ -199,17 +202,18 @@ __host__ __device__ __forceinline__ void scale_principal32(M2f &H, const Inv32 &
     H.a11 = h.a11 + (m11 + (m01 * h.a01 + m11 * h.a11));
 }
 
-__host__ __device__ __forceinline__ int dp_map32(const Consts32 &k, M2f &H, float &Jp_inv, const Inv32 &v, float p,
+__host__ __device__ __forceinline__ int dp_map32(const Consts32 &k, M2f &H, float &jpm1, const Inv32 &v, float p,
                                                  float q, float rho)
 {
     if (fabsf(p + k.p_thr) <= kDpMargin * fmaxf(k.p_thr, fabsf(p)) || fabsf(p - k.dp_pmax) <= kDpMargin * k.dp_pmax)
         return kC32_NEEDS_FP64;
     const float e0 = v.me + rho, e1 = v.me - rho;
     float d0, d1;  // r_i^2 - 1
-    if (p < -k.p_thr || Jp_inv < 1.0f) {
+    if (p < -k.p_thr || jpm1 < 0.0f) {
         d0 = (k.je_new_m1 - e0) / (1.0f + e0);
         d1 = (k.je_new_m1 - e1) / (1.0f + e1);
-        Jp_inv *= k.je_new / v.J;
+        const float fm1 = (k.je_new_m1 - v.Jm1) / v.J;
+        jpm1 = jpm1 + (fm1 + jpm1 * fm1);
     } else {
         const float qn = (p > k.dp_pmax) ? 0.0f : fminf((p + k.p_thr) * k.tan_phi, k.dp_qmax);
         if (!(q >= qn) || !(q > 0.0f)) return kC32_OK;
@@ -224,17 +228,18 @@ __host__ __device__ __forceinline__ int dp_map32(const Consts32 &k, M2f &H, floa
 // ComputePQ and dp_map32 of a crushed particle (kept out of line: crushed
 // particles are few, and the map's values would add to the register
 // pressure of every particle's update). tau is the Kirchhoff stress of the
-// new H; rc is dp_map32's.
-struct Crushed32 { M2f H; float Jp, p, q; Tau32 tau; int rc; };
+// new H; rc is dp_map32's. jpm1 = Jp_inv - 1 (the state keeps Jp_inv in
+// strain form).
+struct Crushed32 { M2f H; float jpm1, p, q; Tau32 tau; int rc; };
 
-static __device__ __noinline__ Crushed32 crushed32(const Consts32 &k, const M2f H, const float Jp)
+static __device__ __noinline__ Crushed32 crushed32(const Consts32 &k, const M2f H, const float jpm1)
 {
-    Crushed32 o{H, Jp, 0.0f, 0.0f, {0.0f, 0.0f, 0.0f}, kC32_OK};
+    Crushed32 o{H, jpm1, 0.0f, 0.0f, {0.0f, 0.0f, 0.0f}, kC32_OK};
     const Inv32 v = invariants32(H, k.mu, k.kappa);
     const float rho = sqrtf(v.hd * v.hd + v.b01 * v.b01);
     o.p = -0.5f * v.s2;
     o.q = 2.0f * v.s1 * rho;
-    o.rc = dp_map32(k, o.H, o.Jp, v, o.p, o.q, rho);
+    o.rc = dp_map32(k, o.H, o.jpm1, v, o.p, o.q, rho);
     if (o.rc == kC32_OK) o.tau = tau32(invariants32(o.H, k.mu, k.kappa));
     return o;
 }
@@ -244,17 +249,18 @@ static __device__ __noinline__ Crushed32 crushed32(const Consts32 &k, const M2f 
 // new H. Returns kC32_NEEDS_FP64 (state untouched) for an intact particle on
 // or outside its failure surface or within kSurfaceMargin of it, for a
 // crushed one near a discontinuity of the map, and for det F <= 0.25.
-__device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTables32 &T, M2f &H, float &Jp_inv,
+// jpm1 = Jp_inv - 1.
+__device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTables32 &T, M2f &H, float &jpm1,
                                               uint32_t meta, float &p_tr, float &q_tr, Tau32 &tau)
 {
     Inv32 v = invariants32(H, k.mu, k.kappa);
     if (!(v.J > 0.25f)) return kC32_NEEDS_FP64;
     const float p = -0.5f * v.s2;
     if (meta32_crushed(meta)) {
-        const Crushed32 o = crushed32(k, H, Jp_inv);
+        const Crushed32 o = crushed32(k, H, jpm1);
         if (o.rc != kC32_OK) return kC32_NEEDS_FP64;
         H = o.H;
-        Jp_inv = o.Jp;
+        jpm1 = o.jpm1;
         p_tr = o.p;
         q_tr = o.q;
         tau = o.tau;
@@ -275,19 +281,19 @@ __device__ __forceinline__ int constitutive32(const Consts32 &k, const GrainTabl
 // FP64 redo of one particle for the cases constitutive32 declines (kept out
 // of line). Takes and returns values: state passed by reference to an
 // out-of-line call would have to live in local memory in the caller's hot
-// loop.
-struct Via64 { M2f H; float Jp, p_tr, q_tr; uint32_t meta; };
+// loop. jpm1 = Jp_inv - 1 in and out.
+struct Via64 { M2f H; float jpm1, p_tr, q_tr; uint32_t meta; };
 
-static __device__ __noinline__ Via64 constitutive32_via64(const icy_SimParams &P, const M2f H, const float Jp_inv,
+static __device__ __noinline__ Via64 constitutive32_via64(const icy_SimParams &P, const M2f H, const float jpm1,
                                                           const uint32_t meta)
 {
     M2d F = {1.0 + (double)H.a00, (double)H.a01, (double)H.a10, 1.0 + (double)H.a11};
-    double jp = Jp_inv, p, q;
+    double jp = 1.0 + (double)jpm1, p, q;
     uint8_t cr = (uint8_t)meta32_crushed(meta);
     constitutive64(P, F, jp, cr, meta32_res(meta), p, q);
     Via64 o;
     o.H = {(float)(F.a00 - 1.0), (float)F.a01, (float)F.a10, (float)(F.a11 - 1.0)};
-    o.Jp = (float)jp;
+    o.jpm1 = (float)(jp - 1.0);
     o.p_tr = (float)p;
     o.q_tr = (float)q;
     o.meta = (meta & 0x00ffffffu) | ((uint32_t)cr << 24);
