@@ -11,11 +11,14 @@ The FP64 forms must track the oracle to rounding (float atomics reorder the
 P2G and force sums, so bit-exactness is out of reach): positions within
 1e-8 h, velocity, Fe and the per-substep force history within 1e-7 of their
 scales, Jp_inv within 1e-9, identical crushed flags (measured: about 1e-12
-after 10,000 substeps). The FP32 form is held to peak indenter force within
-1 % and the 99th percentile of position error within 1e-3 h; its largest
-position error is reported, not asserted (2.2e-3 h after 10,000 substeps on
-the 70k workload: a handful of crushed particles near the indenter). Each
-test prints its errors as one JSON line (prefix PARITY).
+after 10,000 substeps). The FP32 form (fixed-point positions, Jp_inv in
+strain form) is held to the targets with room for float atomics flipping a
+threshold decision: over 10,000 substeps on the 70k workload, every position
+within 1e-3 h, the 99th percentile within 1e-5 h and the peak force within
+1e-4 (measured: 1.0e-7 h, 2.5e-8 h, 8e-8); over 200 substeps on the 1M
+workload, every position within 1e-6 h and the peak force within 1e-5
+(measured: 2.0e-8 h, 7e-8). Each test prints its errors as one JSON line
+(prefix PARITY).
 """
 import json
 import os
@@ -58,7 +61,8 @@ def test_70k_fp64_forms_track_the_oracle_over_10k_substeps():
     _check_fp64(res, "fp64-stepwise", cps)
     _check_fp64(res, "fp64", cps)
     f32 = res["fp32"]
-    assert f32["10000"]["x_p99_h"] <= 1e-3 and f32["force"]["peak_rel"] <= 1e-2, f32
+    assert f32["10000"]["x_max_h"] <= 1e-3 and f32["10000"]["x_p99_h"] <= 1e-5, f32
+    assert f32["force"]["peak_rel"] <= 1e-4, f32
     assert f32["error_word"] == 0
 
 
@@ -71,5 +75,5 @@ def test_1m_forms_track_the_oracle_over_200_substeps():
     _check_fp64(res, "fp64-stepwise", cps)
     _check_fp64(res, "fp64", cps)
     f32 = res["fp32"]
-    assert f32["200"]["x_p99_h"] <= 1e-3 and f32["force"]["peak_rel"] <= 1e-2, f32
+    assert f32["200"]["x_max_h"] <= 1e-6 and f32["force"]["peak_rel"] <= 1e-5, f32
     assert f32["error_word"] == 0
