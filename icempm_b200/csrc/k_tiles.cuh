@@ -461,8 +461,9 @@ static __device__ __noinline__ void harvest_state(const Consts32 &k, const M2f H
     h[5] = __uint_as_float(meta);
 }
 
-// FP32 strain form: position = int16 cell + FP32 fraction, H = Fe - I; meta
-// holds the grain's residues and the crushed flag (grain_meta32).
+// FP32 strain form: position = int16 cell + 32-bit fixed-point fraction,
+// H = Fe - I, Jp = Jp_inv - 1; meta holds the grain's residues and the
+// crushed flag (grain_meta32). The arithmetic is FP32.
 struct Pol32 {
     static constexpr bool kSurrogate = false;
     static constexpr bool kHarvest = true;
